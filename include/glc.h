@@ -1,0 +1,118 @@
+/*
+ * glc.h -- C ABI of libglc: Goldilocks NTT / coset LDE and Poseidon2 Merkle trees on B200 (sm_100a).
+ *
+ * Each entry point replaces one function of boojum-cuda's Rust API (matter-labs/zksync-crypto-gpu,
+ * crates/boojum-cuda) and keeps its argument meaning, memory layout and checks, so that a caller
+ * such as shivini can bind it as a drop-in (see INTEGRATION.md for the Rust binding).
+ *
+ * Conventions (as in the reference, SURVEY of crates/boojum-cuda/src/{ntt,poseidon2,context}.rs):
+ *   - All buffers are device memory owned by the caller; field elements are uint64_t in [0, 2^64),
+ *     not necessarily canonical (outputs of this library are canonical).
+ *   - Every call enqueues work on `stream` (a cudaStream_t; NULL = legacy default stream) and
+ *     returns without synchronising.
+ *   - The return value is a cudaError_t value: 0 on success.  Where the reference panics through
+ *     assert! on a contract violation, this library returns cudaErrorInvalidValue (1) without
+ *     launching anything, and glc_last_error_message() describes the violated condition.
+ *   - Column-major matrices: column k starts at base + k * stride.
+ */
+#ifndef GLC_H
+#define GLC_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int glc_status;
+
+/* Message of the last contract violation seen by the calling thread ("" if none). */
+const char *glc_last_error_message(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Context: twiddle and power tables of the current device.
+ * Replaces context::Context::create (crates/boojum-cuda/src/context.rs:171-282).  The coarse
+ * log counts are validated as in the reference (<= 30) and recorded; the B200 layout keeps a
+ * flat bit-reversed twiddle table for sizes up to 2^24 in HBM (128 MiB) plus two-level power
+ * tables for the coset shifts.  Like the reference's __constant__ descriptors, the context is
+ * one per device; creating it again replaces it.  Not thread-safe (same as the reference).
+ */
+glc_status glc_context_create(uint32_t powers_of_w_coarse_log_count, uint32_t powers_of_g_coarse_log_count);
+/* Replaces context::Context::destroy (context.rs:284-296). */
+glc_status glc_context_destroy(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Batched NTT / coset LDE (crates/boojum-cuda/src/ntt.rs).
+ * num_ntts columns of 2^log_n elements; column k of the input starts at
+ * inputs_matrix + inputs_offset + k * stride_between_input_arrays (same for outputs).
+ * bitrev_inputs = false: natural-order input, bit-reversed output ("n2b");
+ * bitrev_inputs = true: bit-reversed input, natural-order output ("b2n").
+ * inverse: inverse transform including the 1/N factor.
+ * log_extension_degree > 0 selects the coset s = 7 * w_{2^(log_n+log_extension_degree)}^coset_index:
+ * forward multiplies coefficient j by s^j before the transform, inverse by s^-j after it.
+ * Sizes: 1 <= log_n <= 24, log_n + log_extension_degree <= 30.
+ */
+/* Replaces ntt::batch_ntt_out_of_place (ntt.rs:294-335); inputs_len/outputs_len are the slice
+ * lengths in elements; the two matrices must differ (ntt.rs:317,320). */
+glc_status glc_batch_ntt_out_of_place(const uint64_t *inputs_matrix, size_t inputs_len, uint64_t *outputs_matrix,
+                                      size_t outputs_len, uint32_t log_n, uint32_t num_ntts, uint32_t inputs_offset,
+                                      uint32_t outputs_offset, uint32_t stride_between_input_arrays,
+                                      uint32_t stride_between_output_arrays, bool bitrev_inputs, bool inverse,
+                                      uint32_t log_extension_degree, uint32_t coset_index, void *stream);
+/* Replaces ntt::batch_ntt_in_place (ntt.rs:338-369). */
+glc_status glc_batch_ntt_in_place(uint64_t *inputs_matrix, size_t inputs_len, uint32_t log_n, uint32_t num_ntts,
+                                  uint32_t inputs_offset, uint32_t stride_between_input_arrays, bool bitrev_inputs,
+                                  bool inverse, uint32_t log_extension_degree, uint32_t coset_index, void *stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Bit reversal of the rows of a column-major matrix (rows a power of two).
+ * Replaces ops_complex::bit_reverse (crates/boojum-cuda/src/ops_complex.rs:309-320) ... */
+glc_status glc_bit_reverse(const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint64_t dst_stride, uint32_t rows,
+                           uint32_t cols, void *stream);
+/* ... and ops_complex::bit_reverse_in_place (ops_complex.rs:322-331). */
+glc_status glc_bit_reverse_in_place(uint64_t *values, uint64_t stride, uint32_t rows, uint32_t cols, void *stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Poseidon2 over Goldilocks, width 12, rate 8, capacity 4 (GLHasher,
+ * crates/boojum-cuda/src/poseidon2.rs:383-441).  Digests are stored [4][count]: element j of
+ * digest i at results[j * count + i].
+ */
+/* Installs the 30 x 12 round constants (round-major) on the current device.  The reference
+ * generates them from boojum at build time (crates/boojum-cuda/build/poseidon2_gl.rs:3,34);
+ * without this call the library uses its built-in placeholder set. */
+glc_status glc_poseidon2_set_round_constants(const uint64_t *round_constants);
+/* Replaces GpuTreeHasher::compute_leaf_hashes (poseidon2.rs:180-226). */
+glc_status glc_poseidon2_compute_leaf_hashes(const uint64_t *values, size_t values_len, uint64_t *results,
+                                             size_t results_len, uint32_t log_rows_per_hash, bool load_intermediate,
+                                             bool store_intermediate, void *stream);
+/* Replaces GpuTreeHasher::compute_node_hashes (poseidon2.rs:228-251). */
+glc_status glc_poseidon2_compute_node_hashes(const uint64_t *values, size_t values_len, uint64_t *results,
+                                             size_t results_len, void *stream);
+/* Replaces GpuTreeHasher::build_merkle_tree_leaves (poseidon2.rs:253-274). */
+glc_status glc_poseidon2_build_merkle_tree_leaves(const uint64_t *values, size_t values_len, uint64_t *results,
+                                                  size_t results_len, uint32_t log_rows_per_hash,
+                                                  bool load_intermediate, bool store_intermediate, void *stream);
+/* Replaces GpuTreeHasher::build_merkle_tree_nodes (poseidon2.rs:276-295); values_len == results_len. */
+glc_status glc_poseidon2_build_merkle_tree_nodes(const uint64_t *values, size_t values_len, uint64_t *results,
+                                                 size_t results_len, uint32_t layers_count, void *stream);
+/* Replaces GpuTreeHasher::build_merkle_tree (poseidon2.rs:297-314); results_len = 2 * 4 * leaves. */
+glc_status glc_poseidon2_build_merkle_tree(const uint64_t *values, size_t values_len, uint64_t *results,
+                                           size_t results_len, uint32_t log_rows_per_hash, uint32_t layers_count,
+                                           void *stream);
+/* Replaces GpuTreeHasher::gather_rows (poseidon2.rs:316-348): values is values_rows x cols with
+ * column stride values_stride; results is (indexes_len << log_rows_per_index) x cols. */
+glc_status glc_poseidon2_gather_rows(const uint32_t *indexes, size_t indexes_len, uint32_t log_rows_per_index,
+                                     const uint64_t *values, uint64_t values_rows, uint64_t values_cols,
+                                     uint64_t values_stride, uint64_t *results, uint64_t results_rows,
+                                     uint64_t results_cols, uint64_t results_stride, void *stream);
+/* Replaces GpuTreeHasher::gather_merkle_paths (poseidon2.rs:350-380). */
+glc_status glc_poseidon2_gather_merkle_paths(const uint32_t *indexes, size_t indexes_len, const uint64_t *values,
+                                             size_t values_len, uint64_t *results, size_t results_len,
+                                             uint32_t layers_count, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GLC_H */

@@ -1,0 +1,74 @@
+"""ctypes binding of libglc.so (the C ABI declared in include/glc.h).
+
+The library must have been built (build.py); loading fails loudly otherwise: there is no CPU
+fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libglc.so")
+
+
+class GlcError(RuntimeError):
+    """A non-zero glc_status: a CUDA error code, or cudaErrorInvalidValue (1) for a violated
+    argument contract (where boojum-cuda would panic through assert!)."""
+
+    def __init__(self, status: int, where: str, message: str):
+        self.status = status
+        super().__init__("%s failed with status %d%s" % (where, status, (": " + message) if message else ""))
+
+
+_lib = None
+
+u64p = C.c_void_p
+u32p = C.c_void_p
+sz = C.c_size_t
+u32 = C.c_uint32
+u64 = C.c_uint64
+vp = C.c_void_p
+b = C.c_bool
+
+SIGNATURES = {
+    "glc_last_error_message": (C.c_char_p, []),
+    "glc_context_create": (C.c_int, [u32, u32]),
+    "glc_context_destroy": (C.c_int, []),
+    "glc_batch_ntt_out_of_place": (C.c_int, [u64p, sz, u64p, sz, u32, u32, u32, u32, u32, u32, b, b, u32, u32, vp]),
+    "glc_batch_ntt_in_place": (C.c_int, [u64p, sz, u32, u32, u32, u32, b, b, u32, u32, vp]),
+    "glc_bit_reverse": (C.c_int, [u64p, u64, u64p, u64, u32, u32, vp]),
+    "glc_bit_reverse_in_place": (C.c_int, [u64p, u64, u32, u32, vp]),
+    "glc_poseidon2_set_round_constants": (C.c_int, [u64p]),
+    "glc_poseidon2_compute_leaf_hashes": (C.c_int, [u64p, sz, u64p, sz, u32, b, b, vp]),
+    "glc_poseidon2_compute_node_hashes": (C.c_int, [u64p, sz, u64p, sz, vp]),
+    "glc_poseidon2_build_merkle_tree_leaves": (C.c_int, [u64p, sz, u64p, sz, u32, b, b, vp]),
+    "glc_poseidon2_build_merkle_tree_nodes": (C.c_int, [u64p, sz, u64p, sz, u32, vp]),
+    "glc_poseidon2_build_merkle_tree": (C.c_int, [u64p, sz, u64p, sz, u32, u32, vp]),
+    "glc_poseidon2_gather_rows": (C.c_int, [u32p, sz, u32, u64p, u64, u64, u64, u64p, u64, u64, u64, vp]),
+    "glc_poseidon2_gather_merkle_paths": (C.c_int, [u32p, sz, u64p, sz, u64p, sz, u32, vp]),
+}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libglc.so is not built (run %s/build.py)" % HERE)
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int, where: str) -> None:
+    if status != 0:
+        msg = lib().glc_last_error_message()
+        raise GlcError(status, where, msg.decode() if msg else "")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args), name)

@@ -1,0 +1,60 @@
+// Internal declarations shared by the translation units of libglc (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "../../include/glc.h"
+
+namespace glc {
+
+// Largest NTT size the twiddle table covers (the reference plans stop at 2^24, ntt.rs:70-169).
+static constexpr uint32_t MAX_LOG_N = 24;
+// Roots of unity are powers of w_{2^30} (OMEGA_LOG_ORDER, crates/boojum-cuda/native/context.cuh:9).
+static constexpr uint32_t OMEGA_LOG_ORDER = 30;
+static constexpr int MAX_DEVICES = 64;
+
+// Device-resident tables of one GPU (the reference keeps the same data in five __constant__
+// descriptors plus device arrays, crates/boojum-cuda/native/context.cu:3-8).
+struct DeviceTables {
+  bool ready = false;
+  uint32_t w_coarse_log = 0, g_coarse_log = 0;  // as passed by the caller (kept for reporting)
+  // Flat bit-reversed twiddles T[x] = w_{2^24}^{bitrev_23(x)}, x < 2^23 (forward) and the same for w^-1.
+  uint64_t *tw_fwd = nullptr, *tw_inv = nullptr;
+  // Two-level power tables: g^j = g_lo[j & 4095] * g_hi[j >> 12] (j < 2^24), same for g^-1;
+  // w_{2^30}^y = w_lo[y & 32767] * w_hi[y >> 15] (y < 2^30).
+  uint64_t *g_lo = nullptr, *g_hi = nullptr, *gi_lo = nullptr, *gi_hi = nullptr;
+  uint64_t *w_lo = nullptr, *w_hi = nullptr;
+  uint64_t inv_sizes[OMEGA_LOG_ORDER + 1] = {};
+};
+
+// Tables of the current device, or nullptr when glc_context_create has not run on it.
+const DeviceTables *current_tables();
+
+// Thread-local message for the last contract violation.
+void set_error(const std::string &msg);
+int fail(const std::string &msg);  // set_error + return cudaErrorInvalidValue
+
+inline int last_launch_error() { return (int)cudaGetLastError(); }
+
+// Round constants: installs rc (30*12 values) on the current device.
+int p2_install_round_constants(const uint64_t *rc);
+bool p2_constants_installed();
+
+// Internal launchers reused by the commitment pipeline (all enqueue on `stream`).
+int ntt_launch(const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_ntts, uint64_t in_stride,
+               uint64_t out_stride, bool bitrev_inputs, bool inverse, uint32_t log_ext, uint32_t coset_idx,
+               cudaStream_t stream, uint32_t l2_chunk_cols);
+int bitrev_launch(const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint64_t dst_stride, uint32_t log_rows,
+                  uint32_t cols, cudaStream_t stream);
+int p2_leaves_launch(const uint64_t *values, uint64_t *results, uint32_t rows, uint64_t cols, uint64_t count,
+                     bool load_intermediate, bool store_intermediate, cudaStream_t stream);
+int p2_nodes_launch(const uint64_t *values, uint64_t *results, uint64_t count, cudaStream_t stream);
+// Node layers of a tree whose leaf layer ([4][leaves]) starts at `layer0`; writes layers 1..layers
+// into the following part of the same buffer (reference layout, poseidon2.rs:276-314).
+int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cudaStream_t stream);
+
+}  // namespace glc

@@ -1,0 +1,456 @@
+// Poseidon2 over Goldilocks (width 12, rate 8, capacity 4, x^7, 4+22+4 rounds) for sm_100a:
+// leaf hashing, node hashing, Merkle trees and query gathers.
+//
+// Replaces boojum-cuda's GLHasher kernels (crates/boojum-cuda/native/poseidon2/gl/*,
+// native/poseidon2/queries.cuh) and GpuTreeHasher (crates/boojum-cuda/src/poseidon2.rs).
+// Design:
+//  * one thread per permutation with the 12-element state in registers; the linear layers are
+//    evaluated lazily on 128-bit accumulators (shift-add only) and reduced once per round, and
+//    the next round's constants are added before that reduction, so a round constant costs no
+//    modular addition;
+//  * round constants live in __constant__ memory (uniform across a warp: one broadcast read);
+//  * Merkle node layers run as fused subtrees: one CTA hashes 2*T children down through
+//    log2(2T) layers in shared memory, so a tree of 2^20 leaves needs 3 launches, not 20.
+#include <algorithm>
+
+#include "glc_field.cuh"
+#include "glc_internal.h"
+
+namespace glc {
+
+static constexpr uint32_t ROUNDS = 30;
+static constexpr uint32_t WIDTH = 12;
+
+__constant__ uint64_t c_rc[ROUNDS][WIDTH] = {
+#include "p2_round_constants_placeholder.inc"
+};
+
+static bool g_rc_installed[MAX_DEVICES];
+
+typedef unsigned __int128 u128;
+
+__device__ __forceinline__ uint64_t red(u128 x) { return reduce128((uint64_t)x, (uint64_t)(x >> 64)); }
+
+__device__ __forceinline__ uint64_t sbox(uint64_t x) {
+  const uint64_t x2 = sqr(x);
+  const uint64_t x3 = mul(x2, x);
+  const uint64_t x4 = sqr(x2);
+  return mul(x3, x4);
+}
+
+// M_E = circ(2 M4, M4, M4) with M4 of eprint 2023/323 Appendix B (poseidon2_gl.cuh:11-25,
+// poseidon2_gl_st.cuh:35-55), evaluated on 128-bit lazy sums (outputs < 2^72).
+__device__ __forceinline__ void external_layer(const uint64_t s[WIDTH], u128 o[WIDTH]) {
+#pragma unroll
+  for (int t = 0; t < WIDTH; t += 4) {
+    const u128 x0 = s[t], x1 = s[t + 1], x2 = s[t + 2], x3 = s[t + 3];
+    const u128 t0 = x0 + x1;
+    const u128 t1 = x2 + x3;
+    const u128 t2 = (x1 << 1) + t1;
+    const u128 t3 = (x3 << 1) + t0;
+    const u128 t4 = (t1 << 2) + t3;
+    const u128 t5 = (t0 << 2) + t2;
+    o[t] = t3 + t5;
+    o[t + 1] = t5;
+    o[t + 2] = t2 + t4;
+    o[t + 3] = t4;
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const u128 acc = o[j] + o[4 + j] + o[8 + j];
+#pragma unroll
+    for (int t = 0; t < WIDTH; t += 4) o[t + j] += acc;
+  }
+}
+
+// M_I = J + diag(2^LOG_MU_MINUS_ONE) (poseidon2_gl_st.cuh:57-65; diagonal from
+// poseidon2_gl_constants.cuh.template:17).
+__device__ __forceinline__ void internal_layer(const uint64_t s[WIDTH], u128 o[WIDTH]) {
+  constexpr uint32_t LOG_MU_MINUS_ONE[WIDTH] = {4, 14, 11, 8, 0, 5, 2, 9, 13, 6, 3, 12};
+  u128 sum = 0;
+#pragma unroll
+  for (int i = 0; i < WIDTH; i++) sum += s[i];
+#pragma unroll
+  for (int i = 0; i < WIDTH; i++) o[i] = sum + ((u128)s[i] << LOG_MU_MINUS_ONE[i]);
+}
+
+// Poseidon2 permutation (poseidon2_gl_st.cu:9-23): M_E, 4 full rounds, 22 partial, 4 full.
+__device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
+  u128 acc[WIDTH];
+  external_layer(s, acc);
+#pragma unroll
+  for (uint32_t r = 0; r < ROUNDS; r++) {
+    const bool full = r < 4 || r >= 26;
+    if (full) {
+#pragma unroll
+      for (int i = 0; i < WIDTH; i++) s[i] = sbox(red(acc[i] + c_rc[r][i]));
+      external_layer(s, acc);
+    } else {
+      s[0] = sbox(red(acc[0] + c_rc[r][0]));
+#pragma unroll
+      for (int i = 1; i < WIDTH; i++) s[i] = red(acc[i]);
+      internal_layer(s, acc);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < WIDTH; i++) s[i] = canon(red(acc[i]));
+}
+
+// Leaf hashes (poseidon2_gl_st.cu:25-59): leaf i absorbs values[(i<<r) + row + col*rows*count]
+// column by column, rows within a column, 8 per permutation into state[0..8) (overwrite),
+// zero-padding the last chunk.  Capacity state[8..12) starts at 0 or is loaded from results.
+__global__ void __launch_bounds__(128) p2_leaves_kernel(const uint64_t *values, uint64_t *results, uint32_t log_rows,
+                                                        uint64_t cols, uint64_t count, bool load_intermediate,
+                                                        bool store_intermediate) {
+  const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= count) return;
+  uint64_t s[WIDTH];
+#pragma unroll
+  for (int i = 0; i < WIDTH; i++) s[i] = 0;
+  if (load_intermediate) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) s[8 + k] = results[gid + k * count];
+  }
+  const uint64_t rows = 1ull << log_rows;
+  const uint64_t total = rows * cols;
+  const uint64_t *v = values + (gid << log_rows);
+  const uint64_t col_stride = rows * count;
+  if (log_rows == 0) {
+    uint64_t off = 0;
+    for (; off + 8 <= total; off += 8) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) s[i] = __ldcs(v + (off + i) * col_stride);
+      permutation(s);
+    }
+    if (off < total) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) s[i] = off + i < total ? __ldcs(v + (off + i) * col_stride) : 0;
+      permutation(s);
+    }
+  } else {
+    for (uint64_t off = 0; off < total; off += 8) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const uint64_t o = off + i;
+        s[i] = o < total ? __ldcs(v + (o & (rows - 1)) + (o >> log_rows) * col_stride) : 0;
+      }
+      permutation(s);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) results[gid + k * count] = canon(store_intermediate ? s[8 + k] : s[k]);
+}
+
+// Node hashes (poseidon2_gl_st.cu:61-82): node i = P2(L0..L3, R0..R3, 0,0,0,0)[0..4] with
+// L, R = digests 2i and 2i+1 of the [4][2*count] input layer.
+__device__ __forceinline__ void hash_node(const uint64_t l[4], const uint64_t r[4], uint64_t out[4]) {
+  uint64_t s[WIDTH];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    s[k] = l[k];
+    s[4 + k] = r[k];
+    s[8 + k] = 0;
+  }
+  permutation(s);
+#pragma unroll
+  for (int k = 0; k < 4; k++) out[k] = s[k];
+}
+
+__global__ void __launch_bounds__(128) p2_nodes_kernel(const uint64_t *values, uint64_t *results, uint64_t count) {
+  const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= count) return;
+  uint64_t l[4], r[4], o[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const ulonglong2 lr = __ldcs(reinterpret_cast<const ulonglong2 *>(values + k * 2 * count) + gid);
+    l[k] = lr.x;
+    r[k] = lr.y;
+  }
+  hash_node(l, r, o);
+#pragma unroll
+  for (int k = 0; k < 4; k++) results[k * count + gid] = o[k];
+}
+
+// Fused node layers: the CTA owns 2*T consecutive children of layer `in` ([4][2*count]) and
+// produces up to `layers` parent layers, the j-th written to out_j ([4][count >> j] at
+// out + offset of layer j).  out points at the first parent layer; each following layer starts
+// right after the previous one (reference tree layout, poseidon2.rs:276-314).
+template <uint32_t T>
+__global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint64_t *out, uint64_t count,
+                                                       uint32_t layers) {
+  __shared__ uint64_t sh[4][T];
+  const uint32_t tid = threadIdx.x;
+  uint64_t layer_count = count;          // nodes in the layer being produced
+  uint64_t node = (uint64_t)blockIdx.x * T + tid;  // this thread's node in that layer
+  uint64_t *dst = out;
+  uint32_t active = T;
+  // first layer: children straight from global memory
+  {
+    uint64_t l[4], r[4], o[4];
+    const bool live = node < layer_count;
+    if (live) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const ulonglong2 lr = __ldcs(reinterpret_cast<const ulonglong2 *>(in + k * 2 * layer_count) + node);
+        l[k] = lr.x;
+        r[k] = lr.y;
+      }
+      hash_node(l, r, o);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        dst[k * layer_count + node] = o[k];
+        sh[k][tid] = o[k];
+      }
+    }
+  }
+  for (uint32_t j = 1; j < layers && active > 1; j++) {
+    __syncthreads();
+    dst += 4 * layer_count;
+    layer_count >>= 1;
+    active >>= 1;
+    node = (uint64_t)blockIdx.x * active + tid;
+    uint64_t o[4];
+    const bool live = tid < active && node < layer_count;
+    if (live) {
+      uint64_t l[4], r[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        l[k] = sh[k][2 * tid];
+        r[k] = sh[k][2 * tid + 1];
+      }
+      hash_node(l, r, o);
+#pragma unroll
+      for (int k = 0; k < 4; k++) dst[k * layer_count + node] = o[k];
+    }
+    __syncthreads();
+    if (live) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) sh[k][tid] = o[k];
+    }
+  }
+}
+
+// gather_rows (queries.cuh:9-19)
+__global__ void p2_gather_rows_kernel(const uint32_t *indexes, uint32_t indexes_count, uint32_t log_rows_per_index,
+                                      const uint64_t *values, uint64_t values_stride, uint64_t *results,
+                                      uint64_t results_stride, uint64_t cols) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t rows_out = (uint64_t)indexes_count << log_rows_per_index;
+  if (t >= rows_out) return;
+  const uint64_t idx = t >> log_rows_per_index, x = t & ((1ull << log_rows_per_index) - 1);
+  const uint64_t src_row = ((uint64_t)indexes[idx] << log_rows_per_index) + x;
+  for (uint64_t c = blockIdx.y; c < cols; c += gridDim.y)
+    results[c * results_stride + t] = values[c * values_stride + src_row];
+}
+
+// gather_merkle_paths (queries.cuh:21-37)
+__global__ void p2_gather_paths_kernel(const uint32_t *indexes, uint32_t indexes_count, const uint64_t *values,
+                                       uint32_t log_leaves, uint64_t *results, uint32_t layers) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= indexes_count) return;
+  const uint32_t col = blockIdx.y, layer = blockIdx.z;
+  if (layer >= layers) return;
+  const uint64_t layer_off = (4ull << (log_leaves + 1)) - (4ull << (log_leaves + 1 - layer));
+  const uint64_t col_off = (uint64_t)col << (log_leaves - layer);
+  const uint64_t hash_idx = (uint64_t)(indexes[idx] >> layer) ^ 1u;
+  results[(uint64_t)layer * indexes_count * 4 + (uint64_t)indexes_count * col + idx] = values[layer_off + col_off + hash_idx];
+}
+
+// ---- launchers ----
+
+int p2_leaves_launch(const uint64_t *values, uint64_t *results, uint32_t log_rows, uint64_t cols, uint64_t count,
+                     bool load_intermediate, bool store_intermediate, cudaStream_t stream) {
+  if (count == 0) return 0;
+  const uint32_t threads = 128;
+  const uint64_t blocks = (count + threads - 1) / threads;
+  if (blocks > 0x7fffffffull) return fail("poseidon2: too many leaves");
+  p2_leaves_kernel<<<(uint32_t)blocks, threads, 0, stream>>>(values, results, log_rows, cols, count, load_intermediate,
+                                                             store_intermediate);
+  return last_launch_error();
+}
+
+int p2_nodes_launch(const uint64_t *values, uint64_t *results, uint64_t count, cudaStream_t stream) {
+  if (count == 0) return 0;
+  const uint32_t threads = 128;
+  const uint64_t blocks = (count + threads - 1) / threads;
+  if (blocks > 0x7fffffffull) return fail("poseidon2: too many nodes");
+  p2_nodes_kernel<<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
+  return last_launch_error();
+}
+
+int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cudaStream_t stream) {
+  constexpr uint32_t T = 128;
+  const uint64_t *in = layer0;
+  uint64_t *out = layer0 + 4 * leaves;
+  uint64_t count = leaves >> 1;  // nodes of the first layer to produce
+  uint32_t remaining = layers;
+  while (remaining > 0) {
+    // one launch covers up to log2(T)+1 layers (T threads -> 1 node)
+    uint32_t l = 1;
+    while (l < remaining && (T >> l) >= 1 && l < 8) l++;
+    const uint64_t blocks = (count + T - 1) / T;
+    if (blocks > 0x7fffffffull) return fail("poseidon2: too many nodes");
+    p2_subtree_kernel<T><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
+    const int e = last_launch_error();
+    if (e) return e;
+    // advance past the l layers just written
+    for (uint32_t j = 0; j < l; j++) {
+      in = out;
+      out += 4 * count;
+      count >>= 1;
+    }
+    remaining -= l;
+  }
+  return 0;
+}
+
+int p2_install_round_constants(const uint64_t *rc) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaMemcpyToSymbol(c_rc, rc, sizeof(uint64_t) * ROUNDS * WIDTH);
+  if (e == cudaSuccess && dev >= 0 && dev < MAX_DEVICES) g_rc_installed[dev] = true;
+  return (int)e;
+}
+
+bool p2_constants_installed() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return dev >= 0 && dev < MAX_DEVICES && g_rc_installed[dev];
+}
+
+}  // namespace glc
+
+using namespace glc;
+
+extern "C" glc_status glc_poseidon2_set_round_constants(const uint64_t *round_constants) {
+  if (!round_constants) return fail("poseidon2: null round constants");
+  return p2_install_round_constants(round_constants);
+}
+
+extern "C" glc_status glc_poseidon2_compute_leaf_hashes(const uint64_t *values, size_t values_len, uint64_t *results,
+                                                        size_t results_len, uint32_t log_rows_per_hash,
+                                                        bool load_intermediate, bool store_intermediate,
+                                                        void *stream) {
+  // poseidon2.rs:188-209
+  if (results_len % 4) return fail("compute_leaf_hashes: results_len must be a multiple of 4");
+  const uint64_t count = results_len / 4;
+  if (log_rows_per_hash >= 32) return fail("compute_leaf_hashes: log_rows_per_hash too large");
+  const uint64_t per = count << log_rows_per_hash;
+  if (per == 0 || values_len % per) return fail("compute_leaf_hashes: values_len must be a multiple of count << log_rows_per_hash");
+  const uint64_t rows = 1ull << log_rows_per_hash;
+  const uint64_t cols = values_len / per;
+  if (store_intermediate && (rows * cols) % 8)
+    return fail("compute_leaf_hashes: a checkpointed column slab must fill whole rate-8 chunks");
+  if (cols > 0xffffffffull || count > 0xffffffffull) return fail("compute_leaf_hashes: sizes exceed u32");
+  return p2_leaves_launch(values, results, log_rows_per_hash, cols, count, load_intermediate, store_intermediate,
+                          (cudaStream_t)stream);
+}
+
+extern "C" glc_status glc_poseidon2_compute_node_hashes(const uint64_t *values, size_t values_len, uint64_t *results,
+                                                        size_t results_len, void *stream) {
+  // poseidon2.rs:233-242
+  if (values_len % 8) return fail("compute_node_hashes: values_len must be a multiple of 8");
+  if (results_len % 4) return fail("compute_node_hashes: results_len must be a multiple of 4");
+  if (values_len != results_len * 2) return fail("compute_node_hashes: values_len must be 2 * results_len");
+  if (results_len / 4 > 0xffffffffull) return fail("compute_node_hashes: too many nodes");
+  return p2_nodes_launch(values, results, results_len / 4, (cudaStream_t)stream);
+}
+
+extern "C" glc_status glc_poseidon2_build_merkle_tree_leaves(const uint64_t *values, size_t values_len,
+                                                             uint64_t *results, size_t results_len,
+                                                             uint32_t log_rows_per_hash, bool load_intermediate,
+                                                             bool store_intermediate, void *stream) {
+  // poseidon2.rs:261-265
+  if (results_len % 4) return fail("build_merkle_tree_leaves: results_len must be a multiple of 4");
+  const uint64_t leaves = results_len / 4;
+  if (leaves == 0 || values_len % leaves) return fail("build_merkle_tree_leaves: values_len must be a multiple of leaves");
+  return glc_poseidon2_compute_leaf_hashes(values, values_len, results, results_len, log_rows_per_hash,
+                                           load_intermediate, store_intermediate, stream);
+}
+
+static int nodes_checked(const uint64_t *values, size_t values_len, uint64_t *results, size_t results_len,
+                         uint32_t layers_count, cudaStream_t stream) {
+  // poseidon2.rs:282-292, applied to every layer; then one fused launch sequence
+  if (layers_count == 0) return 0;
+  size_t len = values_len;
+  for (uint32_t l = 0; l < layers_count; l++) {
+    if (len % 8) return fail("build_merkle_tree_nodes: layer length must be a multiple of 8");
+    const size_t v = len / 8;
+    if (v & (v - 1)) return fail("build_merkle_tree_nodes: layer length must be 8 << layer");
+    len /= 2;
+  }
+  if (values_len != results_len) return fail("build_merkle_tree_nodes: values_len must equal results_len");
+  const uint64_t leaves = values_len / 4;
+  if (values + values_len == results) return p2_tree_nodes_launch(const_cast<uint64_t *>(values), leaves, layers_count, stream);
+  // layers of a tree whose leaves live elsewhere: first layer from `values`, then in place
+  int e = p2_nodes_launch(values, results, leaves / 2, stream);
+  if (e || layers_count == 1) return e;
+  return p2_tree_nodes_launch(results, leaves / 2, layers_count - 1, stream);
+}
+
+extern "C" glc_status glc_poseidon2_build_merkle_tree_nodes(const uint64_t *values, size_t values_len,
+                                                            uint64_t *results, size_t results_len,
+                                                            uint32_t layers_count, void *stream) {
+  return nodes_checked(values, values_len, results, results_len, layers_count, (cudaStream_t)stream);
+}
+
+extern "C" glc_status glc_poseidon2_build_merkle_tree(const uint64_t *values, size_t values_len, uint64_t *results,
+                                                      size_t results_len, uint32_t log_rows_per_hash,
+                                                      uint32_t layers_count, void *stream) {
+  // poseidon2.rs:304-313
+  if (layers_count == 0) return fail("build_merkle_tree: layers_count must be > 0");
+  if (results_len % 8) return fail("build_merkle_tree: results_len must be a multiple of 8");
+  const uint64_t leaves = results_len / 8;
+  if (layers_count - 1 >= 64 || (1ull << (layers_count - 1)) > leaves)
+    return fail("build_merkle_tree: 2^(layers_count-1) must be <= leaves");
+  if (leaves == 0 || values_len % leaves) return fail("build_merkle_tree: values_len must be a multiple of leaves");
+  const size_t half = results_len / 2;
+  int e = glc_poseidon2_build_merkle_tree_leaves(values, values_len, results, half, log_rows_per_hash, false, false,
+                                                 stream);
+  if (e) return e;
+  return nodes_checked(results, half, results + half, half, layers_count - 1, (cudaStream_t)stream);
+}
+
+extern "C" glc_status glc_poseidon2_gather_rows(const uint32_t *indexes, size_t indexes_len,
+                                                uint32_t log_rows_per_index, const uint64_t *values,
+                                                uint64_t values_rows, uint64_t values_cols, uint64_t values_stride,
+                                                uint64_t *results, uint64_t results_rows, uint64_t results_cols,
+                                                uint64_t results_stride, void *stream) {
+  // poseidon2.rs:323-333
+  if (log_rows_per_index >= 32) return fail("gather_rows: log_rows_per_index must be < 32");
+  if (results_cols != values_cols) return fail("gather_rows: result cols must equal values cols");
+  if (results_rows != ((uint64_t)indexes_len << log_rows_per_index))
+    return fail("gather_rows: result rows must be indexes_len << log_rows_per_index");
+  if (indexes_len > 0xffffffffull) return fail("gather_rows: too many indexes");
+  if (values_stride < values_rows || results_stride < results_rows) return fail("gather_rows: stride < rows");
+  if (results_rows == 0 || values_cols == 0) return 0;
+  const uint32_t threads = 128;
+  const uint64_t blocks = (results_rows + threads - 1) / threads;
+  const uint32_t gy = (uint32_t)std::min<uint64_t>(values_cols, 65535);
+  p2_gather_rows_kernel<<<dim3((uint32_t)blocks, gy), threads, 0, (cudaStream_t)stream>>>(
+      indexes, (uint32_t)indexes_len, log_rows_per_index, values, values_stride, results, results_stride, values_cols);
+  return last_launch_error();
+}
+
+extern "C" glc_status glc_poseidon2_gather_merkle_paths(const uint32_t *indexes, size_t indexes_len,
+                                                        const uint64_t *values, size_t values_len, uint64_t *results,
+                                                        size_t results_len, uint32_t layers_count, void *stream) {
+  // poseidon2.rs:357-370
+  if (indexes_len > 0xffffffffull) return fail("gather_merkle_paths: too many indexes");
+  if (values_len % 4) return fail("gather_merkle_paths: values_len must be a multiple of 4");
+  const uint64_t vc = values_len / 4;
+  if (vc == 0 || (vc & (vc - 1))) return fail("gather_merkle_paths: values_len / 4 must be a power of two");
+  const uint32_t log_vc = 63 - __builtin_clzll(vc);
+  if (log_vc == 0) return fail("gather_merkle_paths: tree too small");
+  const uint32_t log_leaves = log_vc - 1;
+  if (layers_count > log_leaves) return fail("gather_merkle_paths: layers_count must be <= log2(leaves)");
+  if ((uint64_t)indexes_len * layers_count * 4 != results_len)
+    return fail("gather_merkle_paths: results_len must be indexes_len * layers_count * 4");
+  if (indexes_len == 0 || layers_count == 0) return 0;
+  const uint32_t threads = 32;
+  const uint32_t blocks = (uint32_t)((indexes_len + threads - 1) / threads);
+  p2_gather_paths_kernel<<<dim3(blocks, 4, layers_count), threads, 0, (cudaStream_t)stream>>>(
+      indexes, (uint32_t)indexes_len, values, log_leaves, results, layers_count);
+  return last_launch_error();
+}
