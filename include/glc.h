@@ -3,9 +3,9 @@
  *
  * Each entry point replaces one function of boojum-cuda's Rust API (matter-labs/zksync-crypto-gpu,
  * crates/boojum-cuda) and keeps its argument meaning, memory layout and checks, so that a caller
- * such as shivini can bind it as a drop-in (see INTEGRATION.md for the Rust binding).
+ * such as shivini can bind it as a drop-in.
  *
- * Conventions (as in the reference, SURVEY of crates/boojum-cuda/src/{ntt,poseidon2,context}.rs):
+ * Conventions (as in the reference, crates/boojum-cuda/src/{ntt,poseidon2,context}.rs):
  *   - All buffers are device memory owned by the caller; field elements are uint64_t in [0, 2^64),
  *     not necessarily canonical (outputs of this library are canonical).
  *   - Every call enqueues work on `stream` (a cudaStream_t; NULL = legacy default stream) and
@@ -111,6 +111,29 @@ glc_status glc_poseidon2_gather_rows(const uint32_t *indexes, size_t indexes_len
 glc_status glc_poseidon2_gather_merkle_paths(const uint32_t *indexes, size_t indexes_len, const uint64_t *values,
                                              size_t values_len, uint64_t *results, size_t results_len,
                                              uint32_t layers_count, void *stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Commitment jobs (no single counterpart in boojum-cuda: this is the sequence shivini runs for one
+ * trace / argument / quotient commitment, crates/shivini/src/data_structures/storage.rs:155-330,
+ * cache.rs:353-418, oracle.rs:62-88, built from the calls above).
+ */
+typedef struct glc_commit_job {
+  const uint64_t *evals;  /* cols columns of 2^log_n natural-order evaluations (device) */
+  uint64_t evals_stride;  /* elements between columns, >= 2^log_n */
+  uint32_t log_n;         /* 1..24 */
+  uint32_t cols;          /* >= 1; extension-field columns count as two adjacent base columns */
+  uint32_t log_lde;       /* log2 of the LDE factor f, 0..4 */
+  uint32_t log_cap;       /* log2 of the cap; log_lde <= log_cap <= log_n + log_lde */
+  uint64_t *monomials;    /* optional (NULL = not kept): cols x 2^log_n natural-order coefficients */
+  uint64_t *lde;          /* f cosets x cols x 2^log_n, coset-major; coset c holds the bit-reversed
+                             evaluations on 7 * w_{f*2^log_n}^bitrev(c) * <w_{2^log_n}> */
+  uint64_t *trees;        /* f subtrees x (2 * 4 * 2^log_n) digests, build_merkle_tree layout,
+                             each with cap 2^(log_cap - log_lde) */
+  uint64_t *cap;          /* [4][2^log_cap]: the subtree caps concatenated coset by coset */
+} glc_commit_job;
+
+/* One commitment on one stream (the plain per-call form). */
+glc_status glc_commit(const glc_commit_job *job, void *stream);
 
 #ifdef __cplusplus
 }

@@ -141,3 +141,19 @@ def test_contract_violations(glc):
         H.build_merkle_tree(zeros_dev(16), zeros_dev(16), 0, None, 0)
     with pytest.raises(glc.GlcError):
         H.build_merkle_tree(zeros_dev(16), zeros_dev(16), 0, None, 3)  # 2^(layers-1) > leaves
+
+
+def test_nodes_unaligned_input(glc, oracle):
+    """A digest layer that starts 8 bytes past a 16-byte boundary takes the 8-byte load path."""
+    count = 1 << 9
+    vals = rand_elems(8 * count + 1, 5)
+    d = to_dev(vals)
+    d_res = zeros_dev(4 * count)
+    glc.GLHasher.compute_node_hashes(d[1:], d_res)
+    assert (canon(from_dev(d_res)) == oracle.nodes(np.ascontiguousarray(vals[1:]))).all()
+    d_tree = zeros_dev(8 * count)
+    glc.GLHasher.build_merkle_tree_nodes(d[1:], d_tree, 3)
+    got = canon(from_dev(d_tree))
+    l1 = oracle.nodes(np.ascontiguousarray(vals[1:]))
+    l2 = oracle.nodes(l1)
+    assert (got[:4 * count] == l1).all() and (got[4 * count:6 * count] == l2).all()

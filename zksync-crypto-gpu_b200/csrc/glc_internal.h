@@ -57,4 +57,7 @@ int p2_nodes_launch(const uint64_t *values, uint64_t *results, uint64_t count, c
 // into the following part of the same buffer (reference layout, poseidon2.rs:276-314).
 int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cudaStream_t stream);
 
+int commit_check(const glc_commit_job &j);
+int commit_enqueue(const glc_commit_job &j, cudaStream_t stream);
+
 }  // namespace glc

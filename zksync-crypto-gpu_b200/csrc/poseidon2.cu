@@ -156,16 +156,30 @@ __device__ __forceinline__ void hash_node(const uint64_t l[4], const uint64_t r[
   for (int k = 0; k < 4; k++) out[k] = s[k];
 }
 
+// Children 2i and 2i+1 of row k of a [4][2*count] layer: one 16-byte load when the layer is
+// 16-byte aligned (always, for layers inside a tree buffer), else two 8-byte loads.
+template <bool ALIGNED>
+__device__ __forceinline__ void load_children(const uint64_t *layer, uint64_t count, uint64_t i, uint64_t l[4],
+                                              uint64_t r[4]) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (ALIGNED) {
+      const ulonglong2 lr = __ldcs(reinterpret_cast<const ulonglong2 *>(layer + k * 2 * count) + i);
+      l[k] = lr.x;
+      r[k] = lr.y;
+    } else {
+      l[k] = __ldcs(layer + k * 2 * count + 2 * i);
+      r[k] = __ldcs(layer + k * 2 * count + 2 * i + 1);
+    }
+  }
+}
+
+template <bool ALIGNED>
 __global__ void __launch_bounds__(128) p2_nodes_kernel(const uint64_t *values, uint64_t *results, uint64_t count) {
   const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= count) return;
   uint64_t l[4], r[4], o[4];
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const ulonglong2 lr = __ldcs(reinterpret_cast<const ulonglong2 *>(values + k * 2 * count) + gid);
-    l[k] = lr.x;
-    r[k] = lr.y;
-  }
+  load_children<ALIGNED>(values, count, gid, l, r);
   hash_node(l, r, o);
 #pragma unroll
   for (int k = 0; k < 4; k++) results[k * count + gid] = o[k];
@@ -175,7 +189,7 @@ __global__ void __launch_bounds__(128) p2_nodes_kernel(const uint64_t *values, u
 // produces up to `layers` parent layers, the j-th written to out_j ([4][count >> j] at
 // out + offset of layer j).  out points at the first parent layer; each following layer starts
 // right after the previous one (reference tree layout, poseidon2.rs:276-314).
-template <uint32_t T>
+template <uint32_t T, bool ALIGNED>
 __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint64_t *out, uint64_t count,
                                                        uint32_t layers) {
   __shared__ uint64_t sh[4][T];
@@ -189,12 +203,7 @@ __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint6
     uint64_t l[4], r[4], o[4];
     const bool live = node < layer_count;
     if (live) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const ulonglong2 lr = __ldcs(reinterpret_cast<const ulonglong2 *>(in + k * 2 * layer_count) + node);
-        l[k] = lr.x;
-        r[k] = lr.y;
-      }
+      load_children<ALIGNED>(in, layer_count, node, l, r);
       hash_node(l, r, o);
 #pragma unroll
       for (int k = 0; k < 4; k++) {
@@ -274,7 +283,10 @@ int p2_nodes_launch(const uint64_t *values, uint64_t *results, uint64_t count, c
   const uint32_t threads = 128;
   const uint64_t blocks = (count + threads - 1) / threads;
   if (blocks > 0x7fffffffull) return fail("poseidon2: too many nodes");
-  p2_nodes_kernel<<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
+  if ((reinterpret_cast<uintptr_t>(values) & 15) == 0)
+    p2_nodes_kernel<true><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
+  else
+    p2_nodes_kernel<false><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
   return last_launch_error();
 }
 
@@ -290,7 +302,10 @@ int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cud
     while (l < remaining && (T >> l) >= 1 && l < 8) l++;
     const uint64_t blocks = (count + T - 1) / T;
     if (blocks > 0x7fffffffull) return fail("poseidon2: too many nodes");
-    p2_subtree_kernel<T><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
+    if ((reinterpret_cast<uintptr_t>(in) & 15) == 0)
+      p2_subtree_kernel<T, true><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
+    else
+      p2_subtree_kernel<T, false><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
     const int e = last_launch_error();
     if (e) return e;
     // advance past the l layers just written
