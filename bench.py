@@ -1,0 +1,381 @@
+"""Benchmark: Goldilocks LDE + Poseidon2 Merkle commitment throughput on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one full commitment of the headline workload (128 columns x 2^20 rows of seeded
+synthetic Goldilocks elements: iNTT to monomials, LDE factor 2, Poseidon2 leaf hashing of every
+row across the 128 columns, node layers up to a cap of 16).  Inputs are resident in HBM when
+the timed region starts (1 GiB, larger than the 126 MB L2).  Rank 0 prints one JSON line.
+
+--impl reference times the reference's CPU algorithm for the same workload on the host cores
+(the oracle's C restatement of boojum's NTT / LDE / Poseidon2 Merkle routines, all threads, a
+bounded sample per step); boojum itself (Rust) cannot be built here.
+Under torchrun each rank runs its own replica (the jobs are independent: weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LOG_N, COLS, LOG_LDE, LOG_CAP = 20, 128, 1, 4
+WORKLOAD = "128 columns x 2^20 rows, iNTT + coset LDE x2 + Poseidon2 Merkle tree (cap 16)"
+SEED = "glc-bench-c2"
+MODMUL_PER_PERM = 472
+
+
+def job_units(log_n=LOG_N, cols=COLS, log_lde=LOG_LDE, log_cap=LOG_CAP):
+    """elements, permutations, algorithmic bytes and modmuls of one commitment."""
+    n, f = 1 << log_n, 1 << log_lde
+    perms_leaves = f * n * ((cols + 7) // 8)
+    perms_nodes = f * n - (1 << log_cap)
+    bytes_ = 8 * n * cols * (1 + f) + 64 * f * n
+    modmul = cols * (n // 2 * log_n + n) + f * cols * (n + n // 2 * log_n) + MODMUL_PER_PERM * (perms_leaves + perms_nodes)
+    return {"elements": n * cols, "perms_leaves": perms_leaves, "perms_nodes": perms_nodes, "bytes": bytes_,
+            "modmul": modmul}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        loaded = [x for x in sm if mx and x > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(threads=None):
+    """The oracle's commitment (C restatement of the reference algorithm) on a bounded sample
+    of the same workload shape: 128 columns x 2^16 rows, LDE x2, cap 16."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
+    consts = importlib.import_module("zksync-crypto-gpu_b200.p2_constants")
+    O.set_round_constants(consts.env_round_constants() or consts.grain_lfsr_round_constants())
+    threads = threads or os.cpu_count() or 1
+    log_n = 16
+    ev = syn.random_field_elements(SEED + "-cpu", COLS << log_n)
+    t0 = time.perf_counter()
+    O.commit(np.ascontiguousarray(ev), log_n, COLS, LOG_LDE, LOG_CAP, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": (COLS << log_n) / dt, "unit": "elements/s", "cores": threads, "kind": "port",
+            "sample": "128 columns x 2^16 rows (1/16 of the rows), LDE x2, cap 16; %.2f s" % dt, "seconds": dt}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    steps = []
+    for _ in range(args.warmup):
+        cpu_baseline()
+    for _ in range(args.steps):
+        steps.append(cpu_baseline())
+    v = statistics.median(s["value"] for s in steps)
+    ms = statistics.median(s["seconds"] for s in steps) * 1e3
+    cb = dict(steps[0])
+    cb["value"] = v
+    cb.pop("seconds", None)
+    line = {"impl": "reference", "metric": "LDE+Merkle commit elements/s", "value": v, "unit": "elements/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: seeded ChaCha20 Goldilocks elements",
+            "config": {"workload": WORKLOAD, "sample_rows": "2^16 of 2^20 per step (CPU-bounded sample)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "boojum's Rust CPU path cannot be built here (no Rust toolchain); the oracle restates it in C"}
+    print(json.dumps(line), flush=True)
+
+
+def reference_kernels_ms(glc, torch, job, steps):
+    """The reference's own CUDA kernels (boojum-cuda native, compiled for sm_100a) driven with the
+    reference's per-call launch plans on the same workload; None when not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import refkern
+    except Exception:
+        return None
+    if not refkern.available():
+        return None
+    n, f = 1 << LOG_N, 1 << LOG_LDE
+    refkern.call("ref_context_create", 15, 15)
+    s = torch.cuda.current_stream().cuda_stream
+    mono = torch.empty(COLS * n, dtype=torch.int64, device="cuda")
+    layers = LOG_N - (LOG_CAP - LOG_LDE) + 1
+
+    def step():
+        refkern.call("ref_batch_ntt", job.evals.data_ptr(), mono.data_ptr(), LOG_N, COLS, n, n, False, True, 0, 0, s)
+        refkern.call("ref_bit_reverse", mono.data_ptr(), n, mono.data_ptr(), n, LOG_N, COLS, s)
+        for c in range(f):
+            coset = int(format(c, "0%db" % LOG_LDE)[::-1], 2)
+            dst = job.lde.data_ptr() + c * COLS * n * 8
+            refkern.call("ref_batch_ntt", mono.data_ptr(), dst, LOG_N, COLS, n, n, False, False, LOG_LDE, coset, s)
+            refkern.call("ref_p2_build_merkle_tree", dst, COLS * n, job.trees.data_ptr() + c * 8 * n * 8, 8 * n, 0,
+                         layers, s)
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    refkern.call("ref_context_destroy")
+    del mono
+    return e0.elapsed_time(e1) / steps
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    glc = importlib.import_module("zksync-crypto-gpu_b200")
+    syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
+    consts = importlib.import_module("zksync-crypto-gpu_b200.p2_constants")
+    torch.cuda.set_device(local_rank)
+    ctx = glc.Context.create(15, 15)
+    rc = consts.env_round_constants()
+    if rc:
+        glc.poseidon2.set_round_constants(rc)
+    tune_path = os.path.join(ROOT, "zksync-crypto-gpu_b200", "tuning_b200.txt")
+    if os.path.exists(tune_path):
+        glc.tuning.load(tune_path)
+    n, f = 1 << LOG_N, 1 << LOG_LDE
+    sz = glc.CommitJob.sizes(LOG_N, COLS, LOG_LDE, LOG_CAP)
+    dev = lambda k: torch.empty(sz[k], dtype=torch.int64, device="cuda")
+    job = glc.CommitJob(evals=dev("evals"), log_n=LOG_N, cols=COLS, log_lde=LOG_LDE, log_cap=LOG_CAP,
+                        lde=dev("lde"), trees=dev("trees"), cap=dev("cap"), monomials=dev("monomials"))
+    syn.fill_device(job.evals, "%s-rank%d" % (SEED, rank))
+    stream = torch.cuda.current_stream()
+    n_ev = 3 + 3 * f
+    events = [torch.cuda.Event(enable_timing=True) for _ in range(n_ev)]
+    ev_arr = (C.c_void_p * n_ev)(*[e.cuda_event for e in events])
+    jstruct = job._struct()
+    lib = glc._lib.lib()
+
+    def step(profiled):
+        if profiled:
+            glc._lib.check(lib.glc_commit_profiled(C.addressof(jstruct), stream.cuda_stream, ev_arr, n_ev),
+                           "glc_commit_profiled")
+        else:
+            glc._lib.check(lib.glc_commit(C.addressof(jstruct), stream.cuda_stream), "glc_commit")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    barrier()
+    # ---- timed region: inputs resident in HBM ----
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    stage = {"monomials": 0.0, "ntt": 0.0, "leaves": 0.0, "nodes": 0.0, "caps": 0.0}
+    l0 = lib.glc_launch_count()
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t_start.record()
+    for _ in range(args.steps):
+        step(True)
+        torch.cuda.synchronize()  # read the stage events of this step
+        stage["monomials"] += events[0].elapsed_time(events[1])
+        for c in range(f):
+            b = 1 + 3 * c
+            stage["ntt"] += events[b].elapsed_time(events[b + 1])
+            stage["leaves"] += events[b + 1].elapsed_time(events[b + 2])
+            stage["nodes"] += events[b + 2].elapsed_time(events[b + 3])
+        stage["caps"] += events[n_ev - 2].elapsed_time(events[n_ev - 1])
+    t_end.record()
+    torch.cuda.synchronize()
+    launches = (lib.glc_launch_count() - l0) // max(1, args.steps)
+    clk = clocks.stop()
+    barrier()
+    ms = t_start.elapsed_time(t_end) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    units = job_units()
+    value = units["elements"] * world / (ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers ----
+    h_in = torch.empty(sz["evals"], dtype=torch.int64, pin_memory=True)
+    h_in.copy_(job.evals)
+    h_cap = torch.empty(sz["cap"], dtype=torch.int64, pin_memory=True)
+    e_steps = max(1, min(args.steps, 5))
+    for _ in range(2):
+        job.evals.copy_(h_in, non_blocking=True)
+        step(False)
+        h_cap.copy_(job.cap, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e_steps):
+        job.evals.copy_(h_in, non_blocking=True)
+        step(False)
+        h_cap.copy_(job.cap, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": units["elements"] * world / (e2e_ms / 1e3), "unit": "elements/s", "ms_per_step": e2e_ms,
+           "h2d_bytes_per_step": sz["evals"] * 8, "d2h_bytes_per_step": sz["cap"] * 8}
+
+    # ---- modular-multiply peak of this device (roofline denominator for integer kernels) ----
+    blocks = 148 * 32
+    scratch = torch.empty(blocks * 256, dtype=torch.int64, device="cuda")
+    iters = 2048
+    glc._lib.check(lib.glc_modmul_probe(scratch.data_ptr(), blocks, 64, stream.cuda_stream), "probe")
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    glc._lib.check(lib.glc_modmul_probe(scratch.data_ptr(), blocks, iters, stream.cuda_stream), "probe")
+    p1.record()
+    torch.cuda.synchronize()
+    mm_peak = blocks * 256 * 8 * iters / (p0.elapsed_time(p1) / 1e3)
+
+    peaks, peak_kind = measured_peaks()
+    leaf_ms = stage["leaves"] / (args.steps * f)  # per launch
+    leaf_modmul = MODMUL_PER_PERM * units["perms_leaves"] / f
+    achieved = leaf_modmul / (leaf_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as fh:
+            traffic = json.load(fh).get("p2_leaves_kernel_bytes_per_launch")
+    t_roof = max(units["bytes"] / (peaks["hbm_gbs"] * 1e9), units["modmul"] / mm_peak)
+    ref_ms = None
+    if rank == 0 and not args.no_ref_kernels:
+        try:
+            ref_ms = reference_kernels_ms(glc, torch, job, max(1, min(args.steps, 3)))
+        except Exception as ex:  # reported, never fatal
+            ref_ms = None
+            print("reference kernels not timed: %s" % ex, file=sys.stderr)
+    cpu = cpu_baseline() if (rank == 0 and world == 1) else None
+    if cpu:
+        cpu.pop("seconds", None)
+    line = {
+        "metric": "LDE+Merkle commit elements/s",
+        "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic: seeded ChaCha20 uniform Goldilocks elements (glc_fill_random, seed %r)" % SEED,
+        "config": {"workload": WORKLOAD, "columns": COLS, "log_rows": LOG_N, "lde_factor": f, "cap": 1 << LOG_CAP,
+                   "parallelism": "replicas" if world > 1 else "single", "l2": "inputs 1 GiB > 126 MB L2, no flush"},
+        "hashes_per_s": (units["perms_leaves"] + units["perms_nodes"]) * world / (ms / 1e3),
+        "stages_ms": {k: v / args.steps for k, v in stage.items()},
+        "roofline": {"bound": "int", "kernel": "p2_leaves_kernel", "achieved": achieved,
+                     "peak": mm_peak / 1e9, "unit": "Gmodmul/s", "frac": achieved * 1e9 / mm_peak,
+                     "traffic": traffic,
+                     "peak_source": "glc_modmul_probe measured live in this run (8 independent chains per thread)"},
+        "roofline_job": {"bytes": units["bytes"], "modmul": units["modmul"], "t_roof_ms": t_roof * 1e3,
+                         "frac": t_roof * 1e3 / ms, "hbm_gbs": peaks["hbm_gbs"], "hbm_source": peak_kind,
+                         "modmul_peak_gs": mm_peak / 1e9},
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    if ref_ms:
+        line["reference_kernels_sm100a"] = {"ms_per_step": ref_ms, "value": units["elements"] / (ref_ms / 1e3),
+                                            "unit": "elements/s", "speedup": ref_ms / ms,
+                                            "what": "boojum-cuda native kernels recompiled for sm_100a, reference launch plans"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.destroy()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-ref-kernels", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

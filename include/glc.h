@@ -135,6 +135,104 @@ typedef struct glc_commit_job {
 /* One commitment on one stream (the plain per-call form). */
 glc_status glc_commit(const glc_commit_job *job, void *stream);
 
+/* glc_commit that also records CUDA events (cudaEvent_t, created by the caller) at the stage
+ * boundaries: events[0] before the first stage, then after the monomials, and for each coset
+ * after its NTT, its leaf hashes and its node layers, then after the cap gather
+ * (n_events >= 3 + 3 * 2^log_lde).  For per-stage timing of a live run. */
+glc_status glc_commit_profiled(const glc_commit_job *job, void *stream, void **events, uint32_t n_events);
+
+/* Many commitments as one unit on `stream`: the jobs run concurrently on n_streams internal
+ * streams (0 = 8), largest first, balanced by estimated cost; `stream` waits for all of them.
+ * Capturable into a CUDA graph. */
+glc_status glc_commit_batch(const glc_commit_job *jobs, uint32_t n_jobs, uint32_t n_streams, void *stream);
+
+/* A batch captured once into a CUDA graph and replayed with one launch.  The graph keeps the
+ * buffer addresses of the jobs it was created with. */
+typedef struct glc_graph glc_graph;
+glc_status glc_commit_graph_create(const glc_commit_job *jobs, uint32_t n_jobs, uint32_t n_streams, glc_graph **out);
+glc_status glc_commit_graph_launch(glc_graph *graph, void *stream);
+glc_status glc_commit_graph_destroy(glc_graph *graph);
+
+/* ---------------------------------------------------------------------------------------------
+ * Serving (no counterpart in boojum-cuda): commitment requests arrive over time; a worker thread
+ * admits them by HBM footprint and in-flight slots and runs them concurrently on a stream pool
+ * (continuous batching).  Host buffers are read and written by the device: pinned memory gives
+ * asynchronous copies.  The context must exist on the device current at glc_server_create.
+ */
+typedef struct glc_server glc_server;
+typedef struct glc_server_config {
+  uint64_t hbm_budget_bytes; /* admission limit on the device memory held by admitted requests */
+  uint32_t max_inflight;     /* at most this many requests on the device at once */
+  uint32_t streams;          /* streams the requests run on (0 = 8) */
+} glc_server_config;
+typedef struct glc_serve_request {
+  const uint64_t *host_evals; /* cols x 2^log_n natural-order evaluations (host) */
+  uint32_t log_n, cols, log_lde, log_cap;
+  uint64_t *host_cap;         /* output: [4][2^log_cap] cap (host) */
+  uint32_t keep_resident;     /* 1: keep the LDE and trees on the device until glc_server_release */
+} glc_serve_request;
+typedef struct glc_serve_result {
+  uint64_t ticket;
+  int status;           /* 0, or the error of this request */
+  double queue_s;       /* submit -> admitted */
+  double latency_s;     /* submit -> result on the host */
+  uint64_t *device_lde; /* keep_resident only: f x cols x 2^log_n, as glc_commit_job.lde */
+  uint64_t *device_trees;
+} glc_serve_result;
+typedef struct glc_server_stats {
+  uint64_t completed, rejected, pending, inflight, used_bytes, peak_bytes, peak_inflight;
+} glc_server_stats;
+glc_status glc_server_create(const glc_server_config *config, glc_server **out);
+/* Rejects (cudaErrorInvalidValue) a request whose footprint exceeds the budget. */
+glc_status glc_server_submit(glc_server *server, const glc_serve_request *request, uint64_t *ticket);
+/* Cancels a request that has not started. */
+glc_status glc_server_cancel(glc_server *server, uint64_t ticket);
+/* Waits up to timeout_s (< 0: forever) for a request; cudaErrorNotReady on timeout. */
+glc_status glc_server_wait(glc_server *server, uint64_t ticket, double timeout_s, glc_serve_result *out);
+/* Frees the device buffers of a finished keep_resident request. */
+glc_status glc_server_release(glc_server *server, uint64_t ticket);
+glc_status glc_server_get_stats(glc_server *server, glc_server_stats *out);
+/* Finishes admitted and pending requests, then frees everything. */
+glc_status glc_server_destroy(glc_server *server);
+
+/* ---------------------------------------------------------------------------------------------
+ * Launch tuning (no counterpart in boojum-cuda, whose plans are fixed tables, ntt.rs:70-169).
+ * Values are per device; glc_autotune times candidates on the current device and installs the
+ * fastest per NTT size and for the leaf kernel.
+ */
+typedef struct glc_ntt_tuning {
+  uint32_t radix_bits;       /* stages per register round: 2, 3 or 4 */
+  uint32_t k1;               /* stages in the strided pass of a two-pass NTT (0 = log_n / 2) */
+  uint32_t max_log_w;        /* tile rows hold up to 2^max_log_w contiguous elements (<= 5) */
+  uint32_t max_cols_per_cta; /* columns one CTA walks with the same twiddles (1..64) */
+  uint32_t l2_chunk_mb;      /* a two-pass NTT runs both passes per chunk of this many MiB */
+} glc_ntt_tuning;
+typedef struct glc_p2_tuning {
+  uint32_t leaf_threads; /* 64, 128 or 256 */
+  uint32_t rolled;       /* 1: partial rounds in a loop, 0: fully unrolled */
+} glc_p2_tuning;
+glc_status glc_tuning_get_ntt(uint32_t log_n, glc_ntt_tuning *out);
+glc_status glc_tuning_set_ntt(uint32_t log_n, const glc_ntt_tuning *tuning);
+glc_status glc_tuning_get_p2(glc_p2_tuning *out);
+glc_status glc_tuning_set_p2(const glc_p2_tuning *tuning);
+/* Times the candidates for log_n in [log_n_min, log_n_max] on `cols` columns (synchronous;
+ * allocates and frees a scratch buffer of cols << log_n_max elements). */
+glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint32_t cols, uint32_t reps);
+glc_status glc_tuning_save(const char *path);
+glc_status glc_tuning_load(const char *path);
+
+/* ---------------------------------------------------------------------------------------------
+ * Utilities (no counterpart in boojum-cuda).
+ */
+/* Elements offset .. offset+count of the seeded synthetic stream: ChaCha20 (RFC 8439) keyed by
+ * key32, little-endian u64 words, a word >= p redrawn from the nonce-1 stream (uniform in [0, p)). */
+glc_status glc_fill_random(uint64_t *dst, uint64_t count, uint64_t offset, const uint8_t *key32, void *stream);
+/* Number of kernel launches this library has issued in this process (all devices). */
+uint64_t glc_launch_count(void);
+/* Modular-multiply throughput probe: blocks x 256 threads, 8 independent chains of `iters`
+ * multiplies each (scratch: blocks * 256 elements). */
+glc_status glc_modmul_probe(uint64_t *scratch, uint32_t blocks, uint32_t iters, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

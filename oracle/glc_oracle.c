@@ -19,18 +19,21 @@ typedef unsigned __int128 u128;
  * ---------------------------------------------------------------------------------------- */
 uint64_t or_canon(uint64_t a) { return a >= OR_P ? a - OR_P : a; }
 
+/* Branch-free (the carries are data-dependent, so branches would mispredict half the time). */
 uint64_t or_add(uint64_t a, uint64_t b) {
   a = or_canon(a);
   b = or_canon(b);
-  uint64_t s = a + b; /* both < p: a carry means s + 2^64 >= p */
-  if (s < a || s >= OR_P) s -= OR_P;
-  return s;
+  const uint64_t s = a + b; /* both < p: a carry means s + 2^64 >= p */
+  const uint64_t t = s - OR_P;
+  const int use_t = (s < a) | (s >= OR_P);
+  return use_t ? t : s;
 }
 
 uint64_t or_sub(uint64_t a, uint64_t b) {
   a = or_canon(a);
   b = or_canon(b);
-  return a >= b ? a - b : a + (OR_P - b);
+  const uint64_t d = a - b;
+  return a >= b ? d : d + OR_P;
 }
 
 /* 128-bit product reduced with 2^64 = 2^32 - 1 and 2^96 = -1 (mod p). */

@@ -1,0 +1,46 @@
+"""The C-ABI library loads and exports every symbol include/glc.h declares, and argument checks
+that need no device answer on CPU."""
+import ctypes as C
+import os
+import re
+
+from conftest import ROOT, load_package
+
+HEADER = os.path.join(ROOT, "include", "glc.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(glc_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported():
+    g = load_package()
+    lib = C.CDLL(g.LIB_PATH)
+    names = declared_functions()
+    assert len(names) > 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_the_header():
+    g = load_package()
+    bound = set(g._lib.SIGNATURES) | {"glc_server_create", "glc_server_submit", "glc_server_cancel", "glc_server_wait",
+                                      "glc_server_release", "glc_server_get_stats", "glc_server_destroy"}
+    assert set(declared_functions()) <= bound
+
+
+def test_contract_checks_without_a_device():
+    g = load_package()
+    L = g._lib.lib()
+    # log_n = 0 is rejected before any device call (ntt.rs:192)
+    assert L.glc_batch_ntt_in_place(None, 64, 0, 1, 0, 64, False, False, 0, 0, None) == 1
+    assert b"log_n" in L.glc_last_error_message()
+    # offset + n > stride (ntt.rs:350)
+    assert L.glc_batch_ntt_in_place(None, 64, 6, 1, 1, 64, False, False, 0, 0, None) == 1
+    # results_len not a multiple of 4 (poseidon2.rs:190)
+    assert L.glc_poseidon2_compute_leaf_hashes(None, 16, None, 6, 0, False, False, None) == 1
+    assert L.glc_poseidon2_compute_node_hashes(None, 16, None, 4, None) == 1
+    assert L.glc_bit_reverse(None, 8, None, 8, 6, 1, None) == 1  # rows not a power of two
+    assert L.glc_tuning_set_p2(None) == 1

@@ -1,0 +1,136 @@
+"""Commitment jobs (plain, batched, CUDA graph), tuning invariance and the device-side input
+generator, against the oracle."""
+import numpy as np
+import pytest
+
+from conftest import canon, load_package, load_synthetic
+from gpu_util import from_dev, to_dev, zeros_dev
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def glc(round_constants):
+    g = load_package()
+    ctx = g.Context.create(15, 15)
+    g.poseidon2.set_round_constants(round_constants)
+    yield g
+    ctx.destroy()
+
+
+def make_job(glc, syn, log_n, cols, log_lde, log_cap, seed, keep_monomials=True):
+    sz = glc.CommitJob.sizes(log_n, cols, log_lde, log_cap)
+    ev = syn.random_field_elements(seed, sz["evals"])
+    job = glc.CommitJob(evals=to_dev(ev), log_n=log_n, cols=cols, log_lde=log_lde, log_cap=log_cap,
+                        lde=zeros_dev(sz["lde"]), trees=zeros_dev(sz["trees"]), cap=zeros_dev(sz["cap"]),
+                        monomials=zeros_dev(sz["monomials"]) if keep_monomials else None)
+    return job, ev
+
+
+def check_job(oracle, job, ev):
+    mono, lde, trees, cap = oracle.commit(ev, job.log_n, job.cols, job.log_lde, job.log_cap)
+    if job.monomials is not None:
+        assert (canon(from_dev(job.monomials)) == mono).all(), "monomials"
+    assert (canon(from_dev(job.lde)) == lde).all(), "lde"
+    assert (canon(from_dev(job.trees)) == trees).all(), "trees"
+    assert (canon(from_dev(job.cap)) == cap).all(), "cap"
+
+
+@pytest.mark.parametrize("log_n,cols,log_lde,log_cap", [(12, 8, 1, 4), (13, 9, 2, 4), (16, 16, 1, 4), (5, 3, 2, 2),
+                                                         (14, 24, 0, 0), (10, 130, 1, 1)])
+def test_commit_plain(glc, oracle, syn, log_n, cols, log_lde, log_cap):
+    job, ev = make_job(glc, syn, log_n, cols, log_lde, log_cap, "plain-%d-%d" % (log_n, cols))
+    glc.commit.commit(job)
+    check_job(oracle, job, ev)
+
+
+def test_commit_without_monomials(glc, oracle, syn):
+    job, ev = make_job(glc, syn, 12, 8, 2, 4, "nomono", keep_monomials=False)
+    glc.commit.commit(job)
+    check_job(oracle, job, ev)
+
+
+def test_commit_batch_uneven_and_alone(glc, oracle, syn):
+    shapes = [(12, 8, 1), (15, 16, 2), (13, 32, 1), (12, 64, 2), (16, 8, 1), (14, 16, 2), (12, 128, 1)]
+    jobs = [make_job(glc, syn, l, c, e, 4, "batch-%d" % i) for i, (l, c, e) in enumerate(shapes)]
+    glc.commit.commit_batch([j for j, _ in jobs], n_streams=4)
+    for j, ev in jobs:
+        check_job(oracle, j, ev)
+    # the same job alone gives the same bits as in the mix
+    j0, ev0 = make_job(glc, syn, *shapes[1], 4, "batch-1")
+    glc.commit.commit(j0)
+    assert (from_dev(j0.cap) == from_dev(jobs[1][0].cap)).all()
+    assert (from_dev(j0.lde) == from_dev(jobs[1][0].lde)).all()
+
+
+def test_commit_graph_replay(glc, oracle, syn):
+    shapes = [(12, 8, 1), (13, 16, 2), (12, 32, 1)]
+    jobs = [make_job(glc, syn, l, c, e, 4, "graph-%d" % i) for i, (l, c, e) in enumerate(shapes)]
+    g = glc.CommitGraph([j for j, _ in jobs], n_streams=3)
+    g.launch()
+    for j, ev in jobs:
+        check_job(oracle, j, ev)
+        j.cap.zero_()
+        j.lde.zero_()
+    g.launch()
+    for j, ev in jobs:
+        check_job(oracle, j, ev)
+    g.close()
+
+
+def test_commit_contract(glc, syn):
+    job, _ = make_job(glc, syn, 12, 8, 1, 0, "bad")  # cap smaller than the coset count
+    with pytest.raises(glc.GlcError):
+        glc.commit.commit(job)
+    job, _ = make_job(glc, syn, 12, 8, 5, 5, "bad2")  # log_lde > 4
+    with pytest.raises(glc.GlcError):
+        glc.commit.commit(job)
+
+
+@pytest.mark.parametrize("radix,k1,lw,cpc", [(2, 0, 5, 8), (3, 7, 3, 1), (4, 12, 4, 4), (3, 10, 5, 64)])
+def test_ntt_tuning_invariance(glc, oracle, radix, k1, lw, cpc):
+    """Every tuning choice computes the same transform (bit-exact)."""
+    log_n = 20 if k1 != 7 else 14
+    n = 1 << log_n
+    cols = 3
+    saved = glc.tuning.get_ntt(log_n)
+    glc.tuning.set_ntt(log_n, radix, k1, lw, cpc, 8)
+    try:
+        x = syn_x = load_synthetic().random_field_elements("tune-%d" % radix, cols * n)
+        for bitrev_inputs, inverse, e, c in ((False, False, 1, 1), (True, True, 2, 3)):
+            d_in, d_out = to_dev(x), zeros_dev(cols * n)
+            glc.ntt.batch_ntt_out_of_place(d_in, d_out, log_n, cols, 0, 0, n, n, bitrev_inputs, inverse, e, c)
+            assert (canon(from_dev(d_out)) == oracle.batch_ntt(syn_x, log_n, cols, n, n, bitrev_inputs, inverse, e, c)).all()
+    finally:
+        glc.tuning.set_ntt(log_n, saved.radix_bits, saved.k1, saved.max_log_w, saved.max_cols_per_cta, saved.l2_chunk_mb)
+
+
+@pytest.mark.parametrize("threads,rolled", [(64, 0), (128, 1), (256, 0), (256, 1)])
+def test_leaf_tuning_invariance(glc, oracle, threads, rolled):
+    saved = glc.tuning.get_p2()
+    glc.tuning.set_p2(threads, rolled)
+    try:
+        count, cols = 1 << 10, 11
+        vals = load_synthetic().random_field_elements("leaf-tune", cols * count)
+        d_res = zeros_dev(4 * count)
+        glc.GLHasher.compute_leaf_hashes(to_dev(vals), d_res, 0, False, False)
+        assert (canon(from_dev(d_res)) == oracle.leaves(vals, 4 * count, 0)).all()
+    finally:
+        glc.tuning.set_p2(saved.leaf_threads, saved.rolled)
+
+
+def test_autotune_keeps_results(glc, oracle, tmp_path):
+    glc.tuning.autotune(10, 12, cols=4, reps=1)
+    path = str(tmp_path / "tuning.txt")
+    glc.tuning.save(path)
+    glc.tuning.load(path)
+    job, ev = make_job(glc, load_synthetic(), 12, 8, 1, 4, "after-tune")
+    glc.commit.commit(job)
+    check_job(oracle, job, ev)
+
+
+@pytest.mark.parametrize("count,offset", [(1, 0), (1000, 3), (1 << 16, 12345)])
+def test_device_random_matches_python(glc, syn, count, offset):
+    d = zeros_dev(count)
+    syn.fill_device(d, "fill-seed", offset)
+    assert (from_dev(d) == syn.random_field_elements("fill-seed", count, offset)).all()

@@ -47,6 +47,22 @@ SIGNATURES = {
     "glc_poseidon2_build_merkle_tree": (C.c_int, [u64p, sz, u64p, sz, u32, u32, vp]),
     "glc_poseidon2_gather_rows": (C.c_int, [u32p, sz, u32, u64p, u64, u64, u64, u64p, u64, u64, u64, vp]),
     "glc_poseidon2_gather_merkle_paths": (C.c_int, [u32p, sz, u64p, sz, u64p, sz, u32, vp]),
+    "glc_commit": (C.c_int, [vp, vp]),
+    "glc_commit_profiled": (C.c_int, [vp, vp, vp, u32]),
+    "glc_launch_count": (C.c_uint64, []),
+    "glc_commit_batch": (C.c_int, [vp, u32, u32, vp]),
+    "glc_commit_graph_create": (C.c_int, [vp, u32, u32, vp]),
+    "glc_commit_graph_launch": (C.c_int, [vp, vp]),
+    "glc_commit_graph_destroy": (C.c_int, [vp]),
+    "glc_tuning_get_ntt": (C.c_int, [u32, vp]),
+    "glc_tuning_set_ntt": (C.c_int, [u32, vp]),
+    "glc_tuning_get_p2": (C.c_int, [vp]),
+    "glc_tuning_set_p2": (C.c_int, [vp]),
+    "glc_autotune": (C.c_int, [u32, u32, u32, u32]),
+    "glc_tuning_save": (C.c_int, [C.c_char_p]),
+    "glc_tuning_load": (C.c_int, [C.c_char_p]),
+    "glc_fill_random": (C.c_int, [u64p, u64, u64, C.c_char_p, vp]),
+    "glc_modmul_probe": (C.c_int, [u64p, u32, u32, vp]),
 }
 
 

@@ -1,0 +1,97 @@
+"""Commitment jobs: evaluations -> monomials -> coset LDE -> Poseidon2 subtrees -> cap.
+
+The sequence shivini runs around boojum-cuda for one commitment
+(crates/shivini/src/data_structures/storage.rs:155-330, cache.rs:353-418), as one call
+(glc_commit), as a batch of uneven jobs on concurrent streams (glc_commit_batch), or as a
+captured CUDA graph replayed with one launch (CommitGraph).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+from ._buffers import as_slice, stream_handle
+from ._lib import call, lib
+
+
+class _Job(C.Structure):
+    _fields_ = [("evals", C.c_void_p), ("evals_stride", C.c_uint64), ("log_n", C.c_uint32), ("cols", C.c_uint32),
+                ("log_lde", C.c_uint32), ("log_cap", C.c_uint32), ("monomials", C.c_void_p), ("lde", C.c_void_p),
+                ("trees", C.c_void_p), ("cap", C.c_void_p)]
+
+
+@dataclass
+class CommitJob:
+    """Device buffers of one commitment (see glc_commit_job in include/glc.h)."""
+    evals: object
+    log_n: int
+    cols: int
+    log_lde: int
+    log_cap: int
+    lde: object
+    trees: object
+    cap: object
+    monomials: object = None
+    evals_stride: int | None = None
+
+    @staticmethod
+    def sizes(log_n: int, cols: int, log_lde: int, log_cap: int) -> dict:
+        n, f = 1 << log_n, 1 << log_lde
+        return {"evals": cols * n, "lde": f * cols * n, "trees": f * 8 * n, "cap": 4 << log_cap, "monomials": cols * n}
+
+    def _struct(self) -> _Job:
+        n = 1 << self.log_n
+        sz = self.sizes(self.log_n, self.cols, self.log_lde, self.log_cap)
+        stride = n if self.evals_stride is None else self.evals_stride
+        ep, el = as_slice(self.evals)
+        lp, ll = as_slice(self.lde)
+        tp, tl = as_slice(self.trees)
+        cp, cl = as_slice(self.cap)
+        if el < (self.cols - 1) * stride + n or ll < sz["lde"] or tl < sz["trees"] or cl < sz["cap"]:
+            raise ValueError("commit: a buffer is shorter than the job needs")
+        mp = None
+        if self.monomials is not None:
+            mp, ml = as_slice(self.monomials)
+            if ml < sz["monomials"]:
+                raise ValueError("commit: monomials buffer too short")
+        return _Job(ep, stride, self.log_n, self.cols, self.log_lde, self.log_cap, mp, lp, tp, cp)
+
+
+def commit(job: CommitJob, stream=None) -> None:
+    """One commitment on one stream (glc_commit)."""
+    s = job._struct()
+    call("glc_commit", C.addressof(s), stream_handle(stream))
+
+
+def _array(jobs):
+    arr = (_Job * len(jobs))(*[j._struct() for j in jobs])
+    return arr
+
+
+def commit_batch(jobs: list[CommitJob], n_streams: int = 0, stream=None) -> None:
+    """Many commitments as one unit on `stream` (glc_commit_batch)."""
+    arr = _array(jobs)
+    call("glc_commit_batch", C.addressof(arr) if jobs else None, len(jobs), n_streams, stream_handle(stream))
+
+
+class CommitGraph:
+    """A batch captured once into a CUDA graph (glc_commit_graph_*); replay with launch()."""
+
+    def __init__(self, jobs: list[CommitJob], n_streams: int = 0):
+        self._arr = _array(jobs)
+        self._h = C.c_void_p()
+        call("glc_commit_graph_create", C.addressof(self._arr), len(jobs), n_streams, C.byref(self._h))
+
+    def launch(self, stream=None) -> None:
+        call("glc_commit_graph_launch", self._h, stream_handle(stream))
+
+    def close(self) -> None:
+        if self._h:
+            call("glc_commit_graph_destroy", self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,181 @@
+// Autotuner: per device, times candidate launch configurations of the NTT (radix bits per
+// register round, stages in the strided pass, tile width, columns per CTA, L2 chunk size) for
+// each size, and of the Poseidon2 leaf kernel (threads per CTA, rolled or unrolled partial
+// rounds), installs the fastest, and saves / loads the table as text.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "glc_internal.h"
+
+namespace glc {
+
+static float time_ms(cudaStream_t s, int reps, const std::function<int()> &fn, int *err) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  *err = fn();  // warm-up
+  cudaEventRecord(a, s);
+  for (int i = 0; i < reps && !*err; i++) *err = fn();
+  cudaEventRecord(b, s);
+  cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return reps ? ms / reps : ms;
+}
+
+}  // namespace glc
+
+using namespace glc;
+
+extern "C" glc_status glc_tuning_get_ntt(uint32_t log_n, glc_ntt_tuning *out) {
+  if (!out || log_n < 1 || log_n > MAX_LOG_N) return fail("tuning: bad arguments");
+  const NttTuning &t = ntt_tuning(log_n);
+  *out = {t.radix_bits, t.k1, t.max_log_w, t.max_cols_per_cta, t.l2_chunk_mb};
+  return 0;
+}
+
+extern "C" glc_status glc_tuning_set_ntt(uint32_t log_n, const glc_ntt_tuning *in) {
+  if (!in || log_n < 1 || log_n > MAX_LOG_N) return fail("tuning: bad arguments");
+  if (in->radix_bits < 2 || in->radix_bits > 4) return fail("tuning: radix_bits must be 2, 3 or 4");
+  if (in->max_log_w > 5 || in->max_cols_per_cta == 0 || in->max_cols_per_cta > 64 || in->l2_chunk_mb == 0)
+    return fail("tuning: values out of range");
+  if (in->k1 && (in->k1 > 12 || log_n - in->k1 > 12 || in->k1 >= log_n)) return fail("tuning: k1 out of range");
+  NttTuning &t = ntt_tuning(log_n);
+  t.radix_bits = in->radix_bits;
+  t.k1 = in->k1;
+  t.max_log_w = in->max_log_w;
+  t.max_cols_per_cta = in->max_cols_per_cta;
+  t.l2_chunk_mb = in->l2_chunk_mb;
+  return 0;
+}
+
+extern "C" glc_status glc_tuning_get_p2(glc_p2_tuning *out) {
+  if (!out) return fail("tuning: bad arguments");
+  const P2Tuning &t = p2_tuning();
+  *out = {t.leaf_threads, t.rolled ? 1u : 0u};
+  return 0;
+}
+
+extern "C" glc_status glc_tuning_set_p2(const glc_p2_tuning *in) {
+  if (!in || (in->leaf_threads != 64 && in->leaf_threads != 128 && in->leaf_threads != 256))
+    return fail("tuning: leaf_threads must be 64, 128 or 256");
+  P2Tuning &t = p2_tuning();
+  t.leaf_threads = in->leaf_threads;
+  t.rolled = in->rolled != 0;
+  return 0;
+}
+
+extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint32_t cols, uint32_t reps) {
+  if (log_n_min < 1 || log_n_max > MAX_LOG_N || log_n_min > log_n_max || cols == 0)
+    return fail("autotune: bad size range");
+  if (!current_tables()) return fail("autotune: glc_context_create has not been called on this device");
+  if (reps == 0) reps = 3;
+  const uint64_t max_elems = (uint64_t)cols << log_n_max;
+  uint64_t *buf = nullptr;
+  cudaError_t ce = cudaMalloc(&buf, std::max<uint64_t>(max_elems, 1ull << 22) * sizeof(uint64_t));
+  if (ce != cudaSuccess) return (int)ce;
+  cudaStream_t s;
+  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  cudaMemsetAsync(buf, 0x5a, std::max<uint64_t>(max_elems, 1ull << 22) * sizeof(uint64_t), s);
+  int err = 0;
+  for (uint32_t log_n = log_n_min; log_n <= log_n_max && !err; log_n++) {
+    const NttTuning saved = ntt_tuning(log_n);
+    NttTuning best = saved;
+    float best_ms = 1e30f;
+    std::vector<uint32_t> k1s = {0};
+    if (log_n > 12)
+      for (uint32_t k = std::max(log_n - 12, 1u); k <= std::min(12u, log_n - 1); k++) k1s.push_back(k);
+    for (uint32_t rb : {2u, 3u, 4u})
+      for (uint32_t k1 : k1s)
+        for (uint32_t lw : {3u, 4u, 5u})
+          for (uint32_t cpc : {1u, 4u, 8u}) {
+            NttTuning c = saved;
+            c.radix_bits = rb;
+            c.k1 = k1;
+            c.max_log_w = lw;
+            c.max_cols_per_cta = cpc;
+            ntt_tuning(log_n) = c;
+            // time a forward coset LDE (the commitment's dominant NTT), in place
+            const float ms = time_ms(s, (int)reps, [&] {
+              return ntt_launch(buf, buf, log_n, cols, 1ull << log_n, 1ull << log_n, false, false, 1, 1, s, 0);
+            }, &err);
+            if (err) break;
+            if (ms < best_ms) {
+              best_ms = ms;
+              best = c;
+            }
+          }
+    ntt_tuning(log_n) = err ? saved : best;
+  }
+  if (!err) {
+    // Poseidon2 leaves: 2^18 rows x 16 columns
+    const uint64_t count = 1ull << 18;
+    const P2Tuning saved = p2_tuning();
+    P2Tuning best = saved;
+    float best_ms = 1e30f;
+    for (uint32_t th : {128u, 256u})
+      for (bool rolled : {false, true}) {
+        P2Tuning c;
+        c.leaf_threads = th;
+        c.rolled = rolled;
+        p2_tuning() = c;
+        const float ms = time_ms(s, (int)reps, [&] {
+          return p2_leaves_launch(buf, buf + 16 * count, 0, 16, count, false, false, s);
+        }, &err);
+        if (err) break;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = c;
+        }
+      }
+    p2_tuning() = err ? saved : best;
+  }
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  cudaFree(buf);
+  return err;
+}
+
+extern "C" glc_status glc_tuning_save(const char *path) {
+  if (!path) return fail("tuning: null path");
+  FILE *f = fopen(path, "w");
+  if (!f) return fail(std::string("tuning: cannot write ") + path);
+  const P2Tuning &p = p2_tuning();
+  fprintf(f, "p2 %u %u\n", p.leaf_threads, p.rolled ? 1u : 0u);
+  for (uint32_t l = 1; l <= MAX_LOG_N; l++) {
+    const NttTuning &t = ntt_tuning(l);
+    fprintf(f, "ntt %u %u %u %u %u %u\n", l, t.radix_bits, t.k1, t.max_log_w, t.max_cols_per_cta, t.l2_chunk_mb);
+  }
+  fclose(f);
+  return 0;
+}
+
+extern "C" glc_status glc_tuning_load(const char *path) {
+  if (!path) return fail("tuning: null path");
+  FILE *f = fopen(path, "r");
+  if (!f) return fail(std::string("tuning: cannot read ") + path);
+  char kind[8];
+  int e = 0;
+  while (!e && fscanf(f, "%7s", kind) == 1) {
+    if (!strcmp(kind, "p2")) {
+      glc_p2_tuning p;
+      if (fscanf(f, "%u %u", &p.leaf_threads, &p.rolled) != 2) e = fail("tuning: malformed p2 line");
+      else e = glc_tuning_set_p2(&p);
+    } else if (!strcmp(kind, "ntt")) {
+      uint32_t l;
+      glc_ntt_tuning t;
+      if (fscanf(f, "%u %u %u %u %u %u", &l, &t.radix_bits, &t.k1, &t.max_log_w, &t.max_cols_per_cta, &t.l2_chunk_mb) != 6)
+        e = fail("tuning: malformed ntt line");
+      else
+        e = glc_tuning_set_ntt(l, &t);
+    } else {
+      e = fail("tuning: unknown line kind");
+    }
+  }
+  fclose(f);
+  return e;
+}

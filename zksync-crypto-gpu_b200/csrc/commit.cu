@@ -45,16 +45,20 @@ static uint32_t brev_bits(uint32_t x, uint32_t bits) {
   return r;
 }
 
-// Enqueues one job on `stream`.
-int commit_enqueue(const glc_commit_job &j, cudaStream_t stream) {
+int commit_enqueue(const glc_commit_job &j, cudaStream_t stream, cudaEvent_t *events) {
+  uint32_t ev = 0;
+  auto mark = [&]() -> int { return events ? (int)cudaEventRecord(events[ev++], stream) : 0; };
   const uint64_t n = 1ull << j.log_n;
   const uint32_t f = 1u << j.log_lde;
   const uint64_t coset_elems = n * j.cols;
   // monomials: the caller's buffer, or the last coset's LDE buffer (transformed last, in place)
   uint64_t *mono = j.monomials ? j.monomials : j.lde + (uint64_t)(f - 1) * coset_elems;
-  int e = ntt_launch(j.evals, mono, j.log_n, j.cols, j.evals_stride, n, false, true, 0, 0, stream, 0);
+  int e = mark();
+  if (e) return e;
+  e = ntt_launch(j.evals, mono, j.log_n, j.cols, j.evals_stride, n, false, true, 0, 0, stream, 0);
   if (e) return e;
   e = bitrev_launch(mono, n, mono, n, j.log_n, j.cols, stream);
+  if (!e) e = mark();
   if (e) return e;
   const uint32_t log_ccap = j.log_cap - j.log_lde;
   const uint32_t layers = j.log_n - log_ccap + 1;
@@ -62,24 +66,39 @@ int commit_enqueue(const glc_commit_job &j, cudaStream_t stream) {
     uint64_t *dst = j.lde + (uint64_t)c * coset_elems;
     const uint32_t coset = brev_bits(c, j.log_lde);
     e = ntt_launch(mono, dst, j.log_n, j.cols, n, n, false, false, j.log_lde, coset, stream, 0);
+    if (!e) e = mark();
     if (e) return e;
     uint64_t *tree = j.trees + (uint64_t)c * 8 * n;
     e = p2_leaves_launch(dst, tree, 0, j.cols, n, false, false, stream);
+    if (!e) e = mark();
     if (e) return e;
     if (layers > 1) {
       e = p2_tree_nodes_launch(tree, n, layers - 1, stream);
       if (e) return e;
     }
+    e = mark();
+    if (e) return e;
   }
   const uint32_t ccap = 1u << log_ccap;
   const uint32_t total = 4 * ccap * f;
   gather_caps_kernel<<<(total + 127) / 128, 128, 0, stream>>>(j.trees, 8 * n, 8 * n - 8ull * ccap, ccap, f, j.cap);
-  return last_launch_error();
+  e = last_launch_error();
+  if (!e) e = mark();
+  return e;
 }
 
 }  // namespace glc
 
 using namespace glc;
+
+extern "C" glc_status glc_commit_profiled(const glc_commit_job *job, void *stream, void **events, uint32_t n_events) {
+  if (!job || !events) return fail("commit: null job or events");
+  int e = commit_check(*job);
+  if (e) return e;
+  if (n_events < 3 + 3 * (1u << job->log_lde)) return fail("commit: need 3 + 3 * 2^log_lde events");
+  if (!current_tables()) return fail("commit: glc_context_create has not been called on this device");
+  return commit_enqueue(*job, (cudaStream_t)stream, reinterpret_cast<cudaEvent_t *>(events));
+}
 
 extern "C" glc_status glc_commit(const glc_commit_job *job, void *stream) {
   if (!job) return fail("commit: null job");

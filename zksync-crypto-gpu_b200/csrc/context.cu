@@ -5,6 +5,7 @@
 // held in __constant__ descriptors; here the hot NTT twiddles are one flat bit-reversed table in
 // HBM (the prefix an NTT of size N touches, N/2 entries, stays in the 126 MB L2), and only the
 // coset shifts use two-level tables.
+#include <atomic>
 #include <vector>
 
 #include "glc_field.cuh"
@@ -13,6 +14,10 @@
 namespace glc {
 
 static thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launches_issued() { return g_launches.load(std::memory_order_relaxed); }
 static DeviceTables g_tables[MAX_DEVICES];
 static std::mutex g_tables_mutex;
 
@@ -64,6 +69,8 @@ using namespace glc;
 
 extern "C" const char *glc_last_error_message(void) { return g_last_error.c_str(); }
 
+extern "C" uint64_t glc_launch_count(void) { return launches_issued(); }
+
 extern "C" glc_status glc_context_create(uint32_t powers_of_w_coarse_log_count, uint32_t powers_of_g_coarse_log_count) {
   // context.rs:175-176
   if (powers_of_w_coarse_log_count > OMEGA_LOG_ORDER || powers_of_g_coarse_log_count > OMEGA_LOG_ORDER)
@@ -106,6 +113,7 @@ extern "C" glc_status glc_context_create(uint32_t powers_of_w_coarse_log_count, 
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = (cudaError_t)ntt_init_device();
   if (e != cudaSuccess) {
     free_tables(t);
     return (int)e;

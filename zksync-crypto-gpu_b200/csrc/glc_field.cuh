@@ -14,48 +14,77 @@ static constexpr uint64_t EPS = 0xFFFFFFFFull;  // 2^64 mod p
 
 __host__ __device__ __forceinline__ uint64_t canon(uint64_t a) { return a >= P ? a - P : a; }
 
-// a + b mod p, inputs and output in [0, 2^64).
-__device__ __forceinline__ uint64_t add(uint64_t a, uint64_t b) {
-  uint64_t s = a + b;
-  if (s < a) {       // wrapped: s + 2^64 = s + EPS
-    s += EPS;
-    if (s < EPS) s += EPS;  // wrapped again (only when s >= p); cannot wrap a third time
-  }
-  return s;
+__device__ __forceinline__ uint32_t lo32(uint64_t x) { return (uint32_t)x; }
+__device__ __forceinline__ uint32_t hi32(uint64_t x) { return (uint32_t)(x >> 32); }
+__device__ __forceinline__ uint64_t pack(uint32_t l, uint32_t h) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(l), "r"(h));
+  return r;
 }
-
-// a - b mod p.
-__device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b) {
-  uint64_t d = a - b;
-  if (a < b) {       // borrowed: d - 2^64 = d - EPS
-    uint64_t e = d - EPS;
-    if (d < EPS) e -= EPS;  // borrowed again
-    d = e;
-  }
+// 32x32 + 64 -> 64 multiply-add (IMAD.WIDE.U32, the fmaheavy pipe)
+__device__ __forceinline__ uint64_t madw(uint32_t a, uint32_t b, uint64_t c) {
+  uint64_t d;
+  asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(d) : "r"(a), "r"(b), "l"(c));
   return d;
 }
 
-// Reduce the 128-bit value hi:lo to [0, 2^64).
-__device__ __forceinline__ uint64_t reduce128(uint64_t lo, uint64_t hi) {
-  const uint64_t hh = hi >> 32;
-  const uint64_t hl = hi & 0xFFFFFFFFull;
-  uint64_t t0 = lo - hh;                 // lo - hh*2^96 == lo + hh*(-1)
-  if (lo < hh) t0 -= EPS;                // borrow: -2^64 = -EPS; t0 >= 2^64 - 2^32 so no new borrow
-  const uint64_t t1 = hl * EPS;          // hl * 2^64 == hl * EPS, < 2^64
-  uint64_t r = t0 + t1;
-  if (r < t1) r += EPS;                  // carry; r <= 2^64 - 2^33 before, so no new carry
-  return r;
+// a + b mod p, inputs and output in [0, 2^64).  A carry out of 64 bits is worth EPS; adding
+// it wraps a second time only when the first wrapped sum is >= p, which adds EPS once more.
+__device__ __forceinline__ uint64_t add(uint64_t a, uint64_t b) {
+  uint32_t r0, r1, c;
+  asm("add.cc.u32 %0, %3, %5;\n\taddc.cc.u32 %1, %4, %6;\n\taddc.u32 %2, 0, 0;"
+      : "=r"(r0), "=r"(r1), "=r"(c)
+      : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+  const uint64_t r = madw(c, 0xFFFFFFFFu, pack(r0, r1));
+  const uint32_t c2 = (c & (r < EPS)) ? 0xFFFFFFFFu : 0u;
+  uint32_t q0, q1;
+  asm("add.cc.u32 %0, %2, %4;\n\taddc.u32 %1, %3, 0;" : "=r"(q0), "=r"(q1) : "r"(lo32(r)), "r"(hi32(r)), "r"(c2));
+  return pack(q0, q1);
 }
 
-// 64x64 -> 128 product from four 32x32->64 multiply-adds.
+// a - b mod p.  A borrow is worth -EPS; subtracting it borrows again only when the wrapped
+// difference is < EPS.
+__device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b) {
+  uint32_t r0, r1, m;
+  asm("sub.cc.u32 %0, %3, %5;\n\tsubc.cc.u32 %1, %4, %6;\n\tsubc.u32 %2, 0, 0;"
+      : "=r"(r0), "=r"(r1), "=r"(m)
+      : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+  uint32_t q0, q1, m2;
+  asm("sub.cc.u32 %0, %3, %5;\n\tsubc.cc.u32 %1, %4, 0;\n\tsubc.u32 %2, 0, 0;"
+      : "=r"(q0), "=r"(q1), "=r"(m2) : "r"(r0), "r"(r1), "r"(m));
+  uint32_t z0, z1;
+  asm("sub.cc.u32 %0, %2, %4;\n\tsubc.u32 %1, %3, 0;" : "=r"(z0), "=r"(z1) : "r"(q0), "r"(q1), "r"(m2));
+  return pack(z0, z1);
+}
+
+// Reduce the 128-bit value hi:lo to [0, 2^64) with carry chains only (ALU pipe):
+//   lo - hh*2^96 == lo - hh;  hl*2^64 == hl*EPS = (hl << 32) - hl;  a carry out is worth EPS.
+__device__ __forceinline__ uint64_t reduce128(uint64_t lo, uint64_t hi) {
+  uint32_t v0, v1;
+  asm("{\n\t"
+      ".reg .u32 t0, t1, m, u0, u1, c;\n\t"
+      "sub.cc.u32 t0, %2, %5;\n\t"   // t = lo - hh
+      "subc.cc.u32 t1, %3, 0;\n\t"
+      "subc.u32 m, 0, 0;\n\t"        // m = borrow ? 0xffffffff : 0
+      "sub.cc.u32 t0, t0, m;\n\t"    // borrow: t -= EPS (t >= 2^64 - 2^32 then: no new borrow)
+      "subc.u32 t1, t1, 0;\n\t"
+      "sub.cc.u32 u0, 0, %4;\n\t"    // u = hl * EPS
+      "subc.u32 u1, %4, 0;\n\t"
+      "add.cc.u32 t0, t0, u0;\n\t"   // r = t + u
+      "addc.cc.u32 t1, t1, u1;\n\t"
+      "addc.u32 c, 0, 0;\n\t"
+      "neg.s32 c, c;\n\t"
+      "add.cc.u32 %0, t0, c;\n\t"    // carry: r += EPS (r <= 2^64 - 2^33 then: no new carry)
+      "addc.u32 %1, t1, 0;\n\t"
+      "}"
+      : "=r"(v0), "=r"(v1)
+      : "r"(lo32(lo)), "r"(hi32(lo)), "r"(lo32(hi)), "r"(hi32(hi)));
+  return pack(v0, v1);
+}
+
+// 64x64 -> 128 product.
 __device__ __forceinline__ void mul_wide(uint64_t a, uint64_t b, uint64_t &lo, uint64_t &hi) {
-  const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
-  const uint32_t b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
-  const uint64_t p00 = (uint64_t)a0 * b0;
-  const uint64_t t = (uint64_t)a1 * b0 + (p00 >> 32);             // < 2^64
-  const uint64_t u = (uint64_t)a0 * b1 + (t & 0xFFFFFFFFull);     // < 2^64
-  hi = (uint64_t)a1 * b1 + (t >> 32) + (u >> 32);                  // <= 2^64 - 1
-  lo = (u << 32) | (p00 & 0xFFFFFFFFull);
+  asm("mul.lo.u64 %0, %2, %3;\n\tmul.hi.u64 %1, %2, %3;" : "=l"(lo), "=l"(hi) : "l"(a), "l"(b));
 }
 
 __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) {
@@ -65,6 +94,15 @@ __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) {
 }
 
 __device__ __forceinline__ uint64_t sqr(uint64_t a) { return mul(a, a); }
+
+// y == A + B * 2^32 (mod p), for A + hi32(B) * EPS < 2^64 - 2^33 (linear-layer accumulators):
+// B * 2^32 = hi32(B) * 2^64 + lo32(B) * 2^32 and 2^64 == EPS.
+__device__ __forceinline__ uint64_t fold(uint64_t A, uint64_t B) {
+  const uint64_t C = madw(hi32(B), 0xFFFFFFFFu, A);
+  uint32_t t, c;
+  asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(t), "=r"(c) : "r"(hi32(C)), "r"(lo32(B)));
+  return madw(c, 0xFFFFFFFFu, pack(lo32(C), t));
+}
 
 __device__ __forceinline__ uint64_t pow(uint64_t a, uint64_t e) {
   uint64_t r = 1;

@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <mutex>
 #include <string>
 
@@ -38,7 +39,31 @@ const DeviceTables *current_tables();
 void set_error(const std::string &msg);
 int fail(const std::string &msg);  // set_error + return cudaErrorInvalidValue
 
-inline int last_launch_error() { return (int)cudaGetLastError(); }
+// Kernel launches issued by this library (process-wide), for benchmark accounting.
+void count_launches(uint64_t n);
+uint64_t launches_issued();
+// Called once after each kernel launch: counts it and returns the launch status.
+inline int last_launch_error() {
+  count_launches(1);
+  return (int)cudaGetLastError();
+}
+
+// Launch choices of the NTT for one size (set by the autotuner, per device and log_n).
+struct NttTuning {
+  uint32_t radix_bits = 3;        // stages per register round: 2, 3 or 4
+  uint32_t k1 = 0;                // stages in the strided pass of a two-pass plan (0: log_n / 2)
+  uint32_t max_log_w = 5;         // at most 2^max_log_w contiguous elements per tile row
+  uint32_t max_cols_per_cta = 8;  // columns one CTA walks with the same twiddles
+  uint32_t l2_chunk_mb = 48;      // columns per L2-resident chunk of a two-pass NTT
+};
+NttTuning &ntt_tuning(uint32_t log_n);
+
+// Launch choices of the Poseidon2 leaf kernel (set by the autotuner, per device).
+struct P2Tuning {
+  uint32_t leaf_threads = 256;  // 64, 128 or 256
+  bool rolled = false;          // partial rounds in a loop (smaller code) or fully unrolled
+};
+P2Tuning &p2_tuning();
 
 // Round constants: installs rc (30*12 values) on the current device.
 int p2_install_round_constants(const uint64_t *rc);
@@ -57,7 +82,12 @@ int p2_nodes_launch(const uint64_t *values, uint64_t *results, uint64_t count, c
 // into the following part of the same buffer (reference layout, poseidon2.rs:276-314).
 int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cudaStream_t stream);
 
+int ntt_init_device();  // kernel attributes; called by glc_context_create
+double job_cost(const glc_commit_job &j);
 int commit_check(const glc_commit_job &j);
-int commit_enqueue(const glc_commit_job &j, cudaStream_t stream);
+// Enqueues one job; when `events` is given, records events[0] before the first stage and one
+// event after each stage: monomials, then per coset {NTT, leaves, nodes}, then the cap gather
+// (2 + 3 * 2^log_lde + 1 events).
+int commit_enqueue(const glc_commit_job &j, cudaStream_t stream, cudaEvent_t *events = nullptr);
 
 }  // namespace glc

@@ -24,7 +24,6 @@
 
 namespace glc {
 
-static constexpr uint32_t RADIX_BITS = 3;
 static constexpr uint32_t MAX_TILE_LOG = 13;  // 8192 elements = 64 KiB of shared memory
 static constexpr uint32_t PASS_THREADS = 512;
 static constexpr uint32_t SINGLE_PASS_MAX_LOG = 12;  // one column per tile, tile + twiddles <= 64 KiB
@@ -100,18 +99,21 @@ __device__ __forceinline__ void radix_round(uint64_t *tile, const uint64_t *tws,
   }
 }
 
-template <bool DIF>
+template <bool DIF, uint32_t RB>
 __device__ __forceinline__ void round_dispatch(uint64_t *tile, const uint64_t *tws, uint32_t k, uint32_t log_w, uint32_t t,
                                                uint32_t r) {
-  if (r == 3)
-    radix_round<3, DIF>(tile, tws, k, log_w, t);
+  if (RB >= 4 && r == 4)
+    radix_round<(RB >= 4 ? 4 : 1), DIF>(tile, tws, k, log_w, t);
+  else if (RB >= 3 && r == 3)
+    radix_round<(RB >= 3 ? 3 : 1), DIF>(tile, tws, k, log_w, t);
   else if (r == 2)
     radix_round<2, DIF>(tile, tws, k, log_w, t);
   else
     radix_round<1, DIF>(tile, tws, k, log_w, t);
 }
 
-__global__ void __launch_bounds__(PASS_THREADS) ntt_pass_kernel(const PassArgs a) {
+template <uint32_t RB>
+__global__ void __launch_bounds__(PASS_THREADS, 2) ntt_pass_kernel(const PassArgs a) {
   extern __shared__ uint64_t smem[];
   const uint32_t k = a.k, log_w = a.log_w;
   const uint32_t E = 1u << (k + log_w);
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__(PASS_THREADS) ntt_pass_kernel(const PassArgs a
   const uint32_t col0 = blockIdx.y * a.cols_per_cta;
   const uint32_t col1 = min(col0 + a.cols_per_cta, a.num_cols);
   const uint32_t wmask = (1u << log_w) - 1;
-  const uint32_t nrounds = (k + RADIX_BITS - 1) / RADIX_BITS;
+  const uint32_t nrounds = (k + RB - 1) / RB;
   for (uint32_t col = col0; col < col1; col++) {
     const uint64_t *src = a.in + (uint64_t)col * a.in_stride;
     uint64_t *dst = a.out + (uint64_t)col * a.out_stride;
@@ -145,14 +147,14 @@ __global__ void __launch_bounds__(PASS_THREADS) ntt_pass_kernel(const PassArgs a
     __syncthreads();
     if (!a.dif) {
       for (uint32_t q = 0; q < nrounds; q++) {
-        const uint32_t t = q * RADIX_BITS;
-        round_dispatch<false>(tile, tws, k, log_w, t, min(RADIX_BITS, k - t));
+        const uint32_t t = q * RB;
+        round_dispatch<false, RB>(tile, tws, k, log_w, t, min(RB, k - t));
         __syncthreads();
       }
     } else {
       for (int q = (int)nrounds - 1; q >= 0; q--) {
-        const uint32_t t = q * RADIX_BITS;
-        round_dispatch<true>(tile, tws, k, log_w, t, min(RADIX_BITS, k - t));
+        const uint32_t t = q * RB;
+        round_dispatch<true, RB>(tile, tws, k, log_w, t, min(RB, k - t));
         __syncthreads();
       }
     }
@@ -215,6 +217,13 @@ __global__ void __launch_bounds__(256) bitrev_tiled_kernel(const uint64_t *src, 
   }
 }
 
+int ntt_init_device() {
+  cudaError_t e = cudaFuncSetAttribute(ntt_pass_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(ntt_pass_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(ntt_pass_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+  return (int)e;
+}
+
 int bitrev_launch(const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint64_t dst_stride, uint32_t log_rows,
                   uint32_t cols, cudaStream_t stream) {
   if (cols == 0) return 0;
@@ -242,11 +251,19 @@ int bitrev_launch(const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint6
 
 // ---- NTT planner ----
 
+NttTuning g_ntt_tuning[MAX_DEVICES][MAX_LOG_N + 1];
+
+NttTuning &ntt_tuning(uint32_t log_n) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return g_ntt_tuning[(dev >= 0 && dev < MAX_DEVICES) ? dev : 0][std::min(log_n, MAX_LOG_N)];
+}
+
 struct Pass {
   uint32_t s0, k, log_w;
 };
 
-static uint32_t make_plan(uint32_t log_n, bool b2n, Pass *passes) {
+static uint32_t make_plan(uint32_t log_n, bool b2n, const NttTuning &tu, Pass *passes) {
   uint32_t ks[2];
   uint32_t np;
   if (log_n <= SINGLE_PASS_MAX_LOG) {
@@ -254,15 +271,18 @@ static uint32_t make_plan(uint32_t log_n, bool b2n, Pass *passes) {
     ks[0] = log_n;
   } else {
     np = 2;
-    ks[0] = log_n / 2;       // strided pass (stages 0 .. k0-1)
-    ks[1] = log_n - ks[0];   // contiguous pass (stages k0 .. L-1)
+    // strided pass (stages 0 .. k0-1) then contiguous pass (stages k0 .. L-1), each <= 12 stages
+    uint32_t k0 = tu.k1 ? tu.k1 : log_n / 2;
+    k0 = std::max(log_n - SINGLE_PASS_MAX_LOG, std::min(k0, SINGLE_PASS_MAX_LOG));
+    ks[0] = k0;
+    ks[1] = log_n - k0;
   }
   Pass p[2];
   for (uint32_t q = 0; q < np; q++) {
     const uint32_t s0 = q == 0 ? 0 : ks[0];
     const uint32_t k = ks[q];
     const uint32_t log_m = log_n - s0 - k;
-    uint32_t log_w = std::min<uint32_t>(MAX_TILE_LOG - k, 5);
+    uint32_t log_w = std::min<uint32_t>(MAX_TILE_LOG - k, tu.max_log_w);
     log_w = std::min(log_w, log_m);
     p[q] = {s0, k, log_w};
   }
@@ -277,19 +297,13 @@ int ntt_launch(const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_n
   const DeviceTables *t = current_tables();
   if (!t) return fail("NTT: glc_context_create has not been called on this device");
   if (num_ntts == 0) return 0;
-  static bool attr_set[MAX_DEVICES] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!attr_set[dev]) {
-    cudaFuncSetAttribute(ntt_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-    attr_set[dev] = true;
-  }
+  const NttTuning &tu = ntt_tuning(log_n);
   Pass passes[2];
-  const uint32_t np = make_plan(log_n, bitrev_inputs, passes);
+  const uint32_t np = make_plan(log_n, bitrev_inputs, tu, passes);
   const uint64_t n = 1ull << log_n;
   if (l2_chunk_cols == 0) {
-    // keep one chunk of columns (about 48 MiB) resident in L2 across the passes
-    const uint64_t budget = 48ull << 20;
+    // keep one chunk of columns resident in L2 across the passes
+    const uint64_t budget = (uint64_t)tu.l2_chunk_mb << 20;
     l2_chunk_cols = (uint32_t)std::max<uint64_t>(1, budget / (n * 8));
   }
   if (np == 1) l2_chunk_cols = num_ntts;
@@ -330,18 +344,26 @@ int ntt_launch(const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_n
       const uint64_t tiles_per_col = n >> tile_log;
       // enough CTAs to fill 148 SMs a few times over; the rest of the columns loop inside a CTA
       const uint64_t want = 148ull * 8;
-      uint32_t cpc = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(8, (tiles_per_col * cols) / want));
+      uint32_t cpc = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tu.max_cols_per_cta, (tiles_per_col * cols) / want));
       a.cols_per_cta = cpc;
       const uint32_t gy = (cols + cpc - 1) / cpc;
       const size_t smem = ((size_t(1) << tile_log) + (size_t(1) << ps.k)) * sizeof(uint64_t);
-      const uint32_t threads = (uint32_t)std::min<uint64_t>(PASS_THREADS, std::max<uint64_t>(32, (1ull << tile_log) >> 3));
+      const uint32_t threads =
+          (uint32_t)std::min<uint64_t>(PASS_THREADS, std::max<uint64_t>(32, (1ull << tile_log) >> tu.radix_bits));
+      if (gy > 65535) count_launches((gy - 1) / 65535);
       for (uint32_t y0 = 0; y0 < gy; y0 += 65535) {
         PassArgs b = a;
         const uint32_t ycount = std::min<uint32_t>(65535, gy - y0);
         b.in += (uint64_t)y0 * cpc * b.in_stride;
         b.out += (uint64_t)y0 * cpc * b.out_stride;
         b.num_cols = std::min<uint32_t>(cols - y0 * cpc, ycount * cpc);
-        ntt_pass_kernel<<<dim3((uint32_t)tiles_per_col, ycount), threads, smem, stream>>>(b);
+        const dim3 grid((uint32_t)tiles_per_col, ycount);
+        if (tu.radix_bits == 2)
+          ntt_pass_kernel<2><<<grid, threads, smem, stream>>>(b);
+        else if (tu.radix_bits == 4)
+          ntt_pass_kernel<4><<<grid, threads, smem, stream>>>(b);
+        else
+          ntt_pass_kernel<3><<<grid, threads, smem, stream>>>(b);
       }
       const int e = last_launch_error();
       if (e) return e;

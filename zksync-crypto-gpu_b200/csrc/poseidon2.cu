@@ -27,10 +27,6 @@ __constant__ uint64_t c_rc[ROUNDS][WIDTH] = {
 
 static bool g_rc_installed[MAX_DEVICES];
 
-typedef unsigned __int128 u128;
-
-__device__ __forceinline__ uint64_t red(u128 x) { return reduce128((uint64_t)x, (uint64_t)(x >> 64)); }
-
 __device__ __forceinline__ uint64_t sbox(uint64_t x) {
   const uint64_t x2 = sqr(x);
   const uint64_t x3 = mul(x2, x);
@@ -38,68 +34,165 @@ __device__ __forceinline__ uint64_t sbox(uint64_t x) {
   return mul(x3, x4);
 }
 
-// M_E = circ(2 M4, M4, M4) with M4 of eprint 2023/323 Appendix B (poseidon2_gl.cuh:11-25,
-// poseidon2_gl_st.cuh:35-55), evaluated on 128-bit lazy sums (outputs < 2^72).
-__device__ __forceinline__ void external_layer(const uint64_t s[WIDTH], u128 o[WIDTH]) {
-#pragma unroll
-  for (int t = 0; t < WIDTH; t += 4) {
-    const u128 x0 = s[t], x1 = s[t + 1], x2 = s[t + 2], x3 = s[t + 3];
-    const u128 t0 = x0 + x1;
-    const u128 t1 = x2 + x3;
-    const u128 t2 = (x1 << 1) + t1;
-    const u128 t3 = (x3 << 1) + t0;
-    const u128 t4 = (t1 << 2) + t3;
-    const u128 t5 = (t0 << 2) + t2;
-    o[t] = t3 + t5;
-    o[t + 1] = t5;
-    o[t + 2] = t2 + t4;
-    o[t + 3] = t4;
-  }
+// ---- M_E = circ(2 M4, M4, M4) (poseidon2_gl_st.cuh:35-55) ----
+// Evaluated as out_t = M4 (x_t + x_0 + x_1 + x_2) on the 32-bit halves of the state with 64-bit
+// accumulators (mad.wide.u32, no carries: the sums stay below 2^39), then folded back to one
+// 64-bit value per element.  `rc` (optional) is added before the fold, which is how the next
+// round's constants enter without a modular addition.
+__device__ __forceinline__ uint64_t kab(uint64_t a, uint32_t k, uint64_t b) {  // k*a + b, small values
+  const uint64_t r = madw(lo32(a), k, b);
+  uint32_t h;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(h) : "r"(hi32(a)), "r"(k), "r"(hi32(r)));
+  return pack(lo32(r), h);
+}
+
+// M4 of eprint 2023/323 Appendix B (poseidon2_gl.cuh:11-25) on accumulators
+__device__ __forceinline__ void m4(uint64_t &x0, uint64_t &x1, uint64_t &x2, uint64_t &x3) {
+  const uint64_t t0 = kab(x0, 1, x1);
+  const uint64_t t1 = kab(x2, 1, x3);
+  const uint64_t t2 = kab(x1, 2, t1);
+  const uint64_t t3 = kab(x3, 2, t0);
+  const uint64_t t4 = kab(t1, 4, t3);
+  const uint64_t t5 = kab(t0, 4, t2);
+  x0 = kab(t3, 1, t5);
+  x1 = t5;
+  x2 = kab(t2, 1, t4);
+  x3 = t4;
+}
+
+// mode 0: no constants; 1: rc[0..12) added; 2: rc[0] added to element 0 only
+template <int MODE>
+__device__ __forceinline__ void external_layer(uint64_t s[WIDTH], const uint64_t *rc) {
+  uint64_t L[WIDTH], H[WIDTH];
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    const u128 acc = o[j] + o[4 + j] + o[8 + j];
+    const uint64_t sl = madw(lo32(s[8 + j]), 1u, madw(lo32(s[4 + j]), 1u, lo32(s[j])));
+    const uint64_t sh = madw(hi32(s[8 + j]), 1u, madw(hi32(s[4 + j]), 1u, hi32(s[j])));
 #pragma unroll
-    for (int t = 0; t < WIDTH; t += 4) o[t + j] += acc;
-  }
-}
-
-// M_I = J + diag(2^LOG_MU_MINUS_ONE) (poseidon2_gl_st.cuh:57-65; diagonal from
-// poseidon2_gl_constants.cuh.template:17).
-__device__ __forceinline__ void internal_layer(const uint64_t s[WIDTH], u128 o[WIDTH]) {
-  constexpr uint32_t LOG_MU_MINUS_ONE[WIDTH] = {4, 14, 11, 8, 0, 5, 2, 9, 13, 6, 3, 12};
-  u128 sum = 0;
-#pragma unroll
-  for (int i = 0; i < WIDTH; i++) sum += s[i];
-#pragma unroll
-  for (int i = 0; i < WIDTH; i++) o[i] = sum + ((u128)s[i] << LOG_MU_MINUS_ONE[i]);
-}
-
-// Poseidon2 permutation (poseidon2_gl_st.cu:9-23): M_E, 4 full rounds, 22 partial, 4 full.
-__device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
-  u128 acc[WIDTH];
-  external_layer(s, acc);
-#pragma unroll
-  for (uint32_t r = 0; r < ROUNDS; r++) {
-    const bool full = r < 4 || r >= 26;
-    if (full) {
-#pragma unroll
-      for (int i = 0; i < WIDTH; i++) s[i] = sbox(red(acc[i] + c_rc[r][i]));
-      external_layer(s, acc);
-    } else {
-      s[0] = sbox(red(acc[0] + c_rc[r][0]));
-#pragma unroll
-      for (int i = 1; i < WIDTH; i++) s[i] = red(acc[i]);
-      internal_layer(s, acc);
+    for (int t = 0; t < 3; t++) {
+      L[4 * t + j] = madw(lo32(s[4 * t + j]), 1u, sl);
+      H[4 * t + j] = madw(hi32(s[4 * t + j]), 1u, sh);
     }
   }
 #pragma unroll
-  for (int i = 0; i < WIDTH; i++) s[i] = canon(red(acc[i]));
+  for (int t = 0; t < 3; t++) {
+    m4(L[4 * t], L[4 * t + 1], L[4 * t + 2], L[4 * t + 3]);
+    m4(H[4 * t], H[4 * t + 1], H[4 * t + 2], H[4 * t + 3]);
+  }
+#pragma unroll
+  for (int i = 0; i < WIDTH; i++) {
+    uint64_t A = L[i], B = H[i];
+    if (MODE == 1 || (MODE == 2 && i == 0)) {
+      A = madw(lo32(rc[i]), 1u, A);
+      B = madw(hi32(rc[i]), 1u, B);
+    }
+    s[i] = fold(A, B);
+  }
+}
+
+// ---- M_I = J + diag(2^LOG_MU_MINUS_ONE) (poseidon2_gl_st.cuh:57-65) ----
+// 96-bit lazy sums with carry chains (ALU pipe: the S-box products already load the IMAD pipe),
+// one 96 -> 64 fold per element.
+struct w96 {
+  uint32_t l0, l1, h;
+};
+__device__ __forceinline__ w96 w_from(uint64_t x) { return {lo32(x), hi32(x), 0u}; }
+__device__ __forceinline__ w96 w_add(w96 a, w96 b) {
+  w96 r;
+  asm("add.cc.u32 %0, %3, %6;\n\taddc.cc.u32 %1, %4, %7;\n\taddc.u32 %2, %5, %8;"
+      : "=r"(r.l0), "=r"(r.l1), "=r"(r.h)
+      : "r"(a.l0), "r"(a.l1), "r"(a.h), "r"(b.l0), "r"(b.l1), "r"(b.h));
+  return r;
+}
+__device__ __forceinline__ w96 w_add64(uint64_t a, uint64_t b) {
+  w96 r;
+  asm("add.cc.u32 %0, %3, %5;\n\taddc.cc.u32 %1, %4, %6;\n\taddc.u32 %2, 0, 0;"
+      : "=r"(r.l0), "=r"(r.l1), "=r"(r.h)
+      : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+  return r;
+}
+__device__ __forceinline__ w96 w_shl64(uint64_t x, int k) {  // x * 2^k, k < 32
+  w96 r;
+  const uint32_t x0 = lo32(x), x1 = hi32(x);
+  r.h = k ? x1 >> (32 - k) : 0u;
+  r.l1 = __funnelshift_l(x0, x1, k);
+  r.l0 = x0 << k;
+  return r;
+}
+// 96 -> 64: h * 2^64 + l == l + h * EPS; one carry correction (h < 2^31)
+__device__ __forceinline__ uint64_t w_red(w96 a) {
+  uint32_t v0, v1;
+  asm("{\n\t.reg .u32 u0, u1, c;\n\t"
+      "sub.cc.u32 u0, 0, %4;\n\tsubc.u32 u1, %4, 0;\n\t"
+      "add.cc.u32 %0, %2, u0;\n\taddc.cc.u32 %1, %3, u1;\n\taddc.u32 c, 0, 0;\n\t"
+      "neg.s32 c, c;\n\tadd.cc.u32 %0, %0, c;\n\taddc.u32 %1, %1, 0;\n\t}"
+      : "=r"(v0), "=r"(v1)
+      : "r"(a.l0), "r"(a.l1), "r"(a.h));
+  return pack(v0, v1);
+}
+
+template <int MODE>
+__device__ __forceinline__ void internal_layer(uint64_t s[WIDTH], const uint64_t *rc) {
+  constexpr int LOG_MU_MINUS_ONE[WIDTH] = {4, 14, 11, 8, 0, 5, 2, 9, 13, 6, 3, 12};
+  w96 sum = w_add64(s[0], s[1]);
+#pragma unroll
+  for (int i = 2; i < WIDTH; i++) sum = w_add(sum, w_from(s[i]));
+#pragma unroll
+  for (int i = 0; i < WIDTH; i++) {
+    w96 v = w_add(sum, w_shl64(s[i], LOG_MU_MINUS_ONE[i]));
+    if (MODE == 1 || (MODE == 2 && i == 0)) v = w_add(v, w_from(rc[i]));
+    s[i] = w_red(v);
+  }
+}
+
+// Poseidon2 permutation (poseidon2_gl_st.cu:9-23): M_E, 4 full rounds, 22 partial, 4 full.
+// Round r's constants are added by the linear layer that precedes it.  ROLLED keeps the 22
+// partial rounds in a loop (smaller code, fewer instruction-cache misses); the autotuner picks.
+template <bool ROLLED>
+__device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
+  external_layer<1>(s, c_rc[0]);
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+#pragma unroll
+    for (int i = 0; i < WIDTH; i++) s[i] = sbox(s[i]);
+    if (r < 3)
+      external_layer<1>(s, c_rc[r + 1]);
+    else
+      external_layer<2>(s, c_rc[4]);
+  }
+  if (ROLLED) {
+#pragma unroll 1
+    for (int r = 4; r < 25; r++) {
+      s[0] = sbox(s[0]);
+      internal_layer<2>(s, c_rc[r + 1]);
+    }
+  } else {
+#pragma unroll
+    for (int r = 4; r < 25; r++) {
+      s[0] = sbox(s[0]);
+      internal_layer<2>(s, c_rc[r + 1]);
+    }
+  }
+  s[0] = sbox(s[0]);
+  internal_layer<1>(s, c_rc[26]);
+#pragma unroll
+  for (int r = 26; r < 30; r++) {
+#pragma unroll
+    for (int i = 0; i < WIDTH; i++) s[i] = sbox(s[i]);
+    if (r < 29)
+      external_layer<1>(s, c_rc[r + 1]);
+    else
+      external_layer<0>(s, nullptr);
+  }
+#pragma unroll
+  for (int i = 0; i < WIDTH; i++) s[i] = canon(s[i]);
 }
 
 // Leaf hashes (poseidon2_gl_st.cu:25-59): leaf i absorbs values[(i<<r) + row + col*rows*count]
 // column by column, rows within a column, 8 per permutation into state[0..8) (overwrite),
 // zero-padding the last chunk.  Capacity state[8..12) starts at 0 or is loaded from results.
-__global__ void __launch_bounds__(128) p2_leaves_kernel(const uint64_t *values, uint64_t *results, uint32_t log_rows,
+template <bool ROLLED>
+__global__ void __launch_bounds__(256) p2_leaves_kernel(const uint64_t *values, uint64_t *results, uint32_t log_rows,
                                                         uint64_t cols, uint64_t count, bool load_intermediate,
                                                         bool store_intermediate) {
   const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -120,12 +213,12 @@ __global__ void __launch_bounds__(128) p2_leaves_kernel(const uint64_t *values, 
     for (; off + 8 <= total; off += 8) {
 #pragma unroll
       for (int i = 0; i < 8; i++) s[i] = __ldcs(v + (off + i) * col_stride);
-      permutation(s);
+      permutation<ROLLED>(s);
     }
     if (off < total) {
 #pragma unroll
       for (int i = 0; i < 8; i++) s[i] = off + i < total ? __ldcs(v + (off + i) * col_stride) : 0;
-      permutation(s);
+      permutation<ROLLED>(s);
     }
   } else {
     for (uint64_t off = 0; off < total; off += 8) {
@@ -134,7 +227,7 @@ __global__ void __launch_bounds__(128) p2_leaves_kernel(const uint64_t *values, 
         const uint64_t o = off + i;
         s[i] = o < total ? __ldcs(v + (o & (rows - 1)) + (o >> log_rows) * col_stride) : 0;
       }
-      permutation(s);
+      permutation<ROLLED>(s);
     }
   }
 #pragma unroll
@@ -143,6 +236,7 @@ __global__ void __launch_bounds__(128) p2_leaves_kernel(const uint64_t *values, 
 
 // Node hashes (poseidon2_gl_st.cu:61-82): node i = P2(L0..L3, R0..R3, 0,0,0,0)[0..4] with
 // L, R = digests 2i and 2i+1 of the [4][2*count] input layer.
+template <bool ROLLED = false>
 __device__ __forceinline__ void hash_node(const uint64_t l[4], const uint64_t r[4], uint64_t out[4]) {
   uint64_t s[WIDTH];
 #pragma unroll
@@ -151,7 +245,7 @@ __device__ __forceinline__ void hash_node(const uint64_t l[4], const uint64_t r[
     s[4 + k] = r[k];
     s[8 + k] = 0;
   }
-  permutation(s);
+  permutation<ROLLED>(s);
 #pragma unroll
   for (int k = 0; k < 4; k++) out[k] = s[k];
 }
@@ -267,14 +361,27 @@ __global__ void p2_gather_paths_kernel(const uint32_t *indexes, uint32_t indexes
 
 // ---- launchers ----
 
+P2Tuning g_p2_tuning[MAX_DEVICES];
+
+P2Tuning &p2_tuning() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return g_p2_tuning[(dev >= 0 && dev < MAX_DEVICES) ? dev : 0];
+}
+
 int p2_leaves_launch(const uint64_t *values, uint64_t *results, uint32_t log_rows, uint64_t cols, uint64_t count,
                      bool load_intermediate, bool store_intermediate, cudaStream_t stream) {
   if (count == 0) return 0;
-  const uint32_t threads = 128;
+  const P2Tuning &tu = p2_tuning();
+  const uint32_t threads = tu.leaf_threads;
   const uint64_t blocks = (count + threads - 1) / threads;
   if (blocks > 0x7fffffffull) return fail("poseidon2: too many leaves");
-  p2_leaves_kernel<<<(uint32_t)blocks, threads, 0, stream>>>(values, results, log_rows, cols, count, load_intermediate,
-                                                             store_intermediate);
+  if (tu.rolled)
+    p2_leaves_kernel<true><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, log_rows, cols, count,
+                                                                     load_intermediate, store_intermediate);
+  else
+    p2_leaves_kernel<false><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, log_rows, cols, count,
+                                                                      load_intermediate, store_intermediate);
   return last_launch_error();
 }
 
@@ -296,6 +403,18 @@ int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cud
   uint64_t *out = layer0 + 4 * leaves;
   uint64_t count = leaves >> 1;  // nodes of the first layer to produce
   uint32_t remaining = layers;
+  // Wide layers: one launch per layer keeps every thread busy.  Once a layer no longer fills
+  // the GPU a few times over, fused subtree launches cover up to 8 layers each, so the narrow
+  // top of the tree costs a handful of launches instead of one per layer.
+  const uint64_t wide = 148ull * 256 * 4;
+  while (remaining > 0 && count >= wide) {
+    const int e = p2_nodes_launch(in, out, count, stream);
+    if (e) return e;
+    in = out;
+    out += 4 * count;
+    count >>= 1;
+    remaining--;
+  }
   while (remaining > 0) {
     // one launch covers up to log2(T)+1 layers (T threads -> 1 node)
     uint32_t l = 1;

@@ -1,0 +1,337 @@
+// Serving runtime: commitment requests arrive over time; a worker thread admits them onto the
+// device by HBM footprint and in-flight slots, runs them concurrently on a pool of streams
+// (continuous batching: a request that arrives while others run starts as soon as memory and a
+// slot free up, and its kernels overlap theirs), and reports per-request latency.
+//
+// Device memory is stream-ordered (cudaMallocAsync / cudaFreeAsync from the device's default
+// memory pool, kept cached between requests), so admission costs no device synchronisation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "glc_internal.h"
+
+namespace glc {
+
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Request {
+  uint64_t ticket = 0;
+  glc_serve_request req{};
+  uint64_t footprint = 0;
+  double t_submit = 0, t_start = 0, t_done = 0;
+  int status = 0;
+  bool started = false, done = false, cancelled = false;
+  int stream = -1;
+  cudaEvent_t done_event = nullptr;
+  uint64_t *d_evals = nullptr, *d_lde = nullptr, *d_trees = nullptr, *d_cap = nullptr;
+};
+
+struct Server {
+  glc_server_config cfg{};
+  int device = 0;
+  std::vector<cudaStream_t> streams;
+  std::vector<uint32_t> stream_load;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<uint64_t> pending;
+  std::map<uint64_t, Request> reqs;
+  uint64_t next_ticket = 1;
+  uint64_t used_bytes = 0;
+  uint32_t inflight = 0;
+  bool stop = false;
+  std::thread worker;
+  // stats
+  uint64_t completed = 0, rejected = 0, peak_bytes = 0;
+  uint32_t peak_inflight = 0;
+};
+
+uint64_t request_footprint(const glc_serve_request &r) {
+  const uint64_t n = 1ull << r.log_n, f = 1ull << r.log_lde;
+  return 8ull * ((uint64_t)r.cols * n * (1 + f) + f * 8 * n + (4ull << r.log_cap));
+}
+
+static int request_check(const glc_serve_request &r) {
+  if (!r.host_evals || !r.host_cap) return fail("serve: null host buffer");
+  glc_commit_job j{};
+  j.evals = reinterpret_cast<const uint64_t *>(1);
+  j.evals_stride = 1ull << std::min(r.log_n, 31u);
+  j.log_n = r.log_n;
+  j.cols = r.cols;
+  j.log_lde = r.log_lde;
+  j.log_cap = r.log_cap;
+  j.lde = j.trees = j.cap = reinterpret_cast<uint64_t *>(1);
+  return commit_check(j);
+}
+
+// Allocates and enqueues one admitted request (worker thread, lock held by the caller).
+static int start_request(Server &s, Request &q) {
+  const glc_serve_request &r = q.req;
+  const uint64_t n = 1ull << r.log_n, f = 1ull << r.log_lde;
+  int best = 0;
+  for (size_t i = 1; i < s.streams.size(); i++)
+    if (s.stream_load[i] < s.stream_load[best]) best = (int)i;
+  q.stream = best;
+  cudaStream_t st = s.streams[best];
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](uint64_t **p, uint64_t elems) {
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)p, elems * sizeof(uint64_t), st);
+  };
+  alloc(&q.d_evals, (uint64_t)r.cols * n);
+  alloc(&q.d_lde, f * r.cols * n);
+  alloc(&q.d_trees, f * 8 * n);
+  alloc(&q.d_cap, 4ull << r.log_cap);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(q.d_evals, r.host_evals, (uint64_t)r.cols * n * 8, cudaMemcpyHostToDevice, st);
+  int err = (int)e;
+  if (!err) {
+    glc_commit_job j{};
+    j.evals = q.d_evals;
+    j.evals_stride = n;
+    j.log_n = r.log_n;
+    j.cols = r.cols;
+    j.log_lde = r.log_lde;
+    j.log_cap = r.log_cap;
+    j.lde = q.d_lde;
+    j.trees = q.d_trees;
+    j.cap = q.d_cap;
+    err = commit_enqueue(j, st);
+  }
+  if (!err) err = (int)cudaMemcpyAsync(r.host_cap, q.d_cap, (4ull << r.log_cap) * 8, cudaMemcpyDeviceToHost, st);
+  if (!err) err = (int)cudaEventCreateWithFlags(&q.done_event, cudaEventDisableTiming);
+  if (!err) err = (int)cudaEventRecord(q.done_event, st);
+  s.stream_load[best]++;
+  return err;
+}
+
+static void free_request(Server &s, Request &q, bool keep_resident) {
+  cudaStream_t st = s.streams[q.stream >= 0 ? q.stream : 0];
+  if (q.d_evals) cudaFreeAsync(q.d_evals, st);
+  if (q.d_cap) cudaFreeAsync(q.d_cap, st);
+  q.d_evals = q.d_cap = nullptr;
+  if (!keep_resident) {
+    if (q.d_lde) cudaFreeAsync(q.d_lde, st);
+    if (q.d_trees) cudaFreeAsync(q.d_trees, st);
+    q.d_lde = q.d_trees = nullptr;
+  }
+  if (q.done_event) cudaEventDestroy(q.done_event);
+  q.done_event = nullptr;
+}
+
+static void worker_main(Server *s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    // admit: FIFO; a request that does not fit lets smaller ones behind it start (backfill)
+    for (auto it = s->pending.begin(); it != s->pending.end() && s->inflight < s->cfg.max_inflight;) {
+      Request &q = s->reqs[*it];
+      if (q.cancelled) {
+        it = s->pending.erase(it);
+        continue;
+      }
+      if (s->used_bytes + q.footprint > s->cfg.hbm_budget_bytes) {
+        ++it;
+        continue;
+      }
+      q.started = true;
+      q.t_start = now_s();
+      s->used_bytes += q.footprint;
+      s->inflight++;
+      s->peak_bytes = std::max(s->peak_bytes, s->used_bytes);
+      s->peak_inflight = std::max(s->peak_inflight, s->inflight);
+      q.status = start_request(*s, q);
+      it = s->pending.erase(it);
+    }
+    // completions
+    bool any_inflight = false;
+    for (auto &kv : s->reqs) {
+      Request &q = kv.second;
+      if (!q.started || q.done) continue;
+      cudaError_t qe = q.status ? cudaSuccess : cudaEventQuery(q.done_event);
+      if (q.status || qe != cudaErrorNotReady) {
+        if (!q.status && qe != cudaSuccess) q.status = (int)qe;
+        q.done = true;
+        q.t_done = now_s();
+        s->stream_load[q.stream]--;
+        free_request(*s, q, q.req.keep_resident && !q.status);
+        if (!(q.req.keep_resident && !q.status)) s->used_bytes -= q.footprint;
+        s->inflight--;
+        s->completed++;
+        s->cv_done.notify_all();
+      } else {
+        any_inflight = true;
+      }
+    }
+    if (s->stop && s->pending.empty() && !any_inflight) break;
+    if (any_inflight)
+      s->cv_work.wait_for(lk, std::chrono::microseconds(50));
+    else
+      s->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+  }
+}
+
+}  // namespace glc
+
+using namespace glc;
+
+struct glc_server {
+  Server s;
+};
+
+extern "C" glc_status glc_server_create(const glc_server_config *config, glc_server **out) {
+  if (!config || !out) return fail("serve: null argument");
+  if (config->max_inflight == 0 || config->hbm_budget_bytes == 0) return fail("serve: zero budget or slots");
+  if (!current_tables()) return fail("serve: glc_context_create has not been called on this device");
+  auto *srv = new glc_server();
+  Server &s = srv->s;
+  s.cfg = *config;
+  if (s.cfg.streams == 0) s.cfg.streams = 8;
+  cudaGetDevice(&s.device);
+  // keep freed blocks in the pool: requests of similar sizes reuse them without new mappings
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, s.device) == cudaSuccess) {
+    uint64_t threshold = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  for (uint32_t i = 0; i < s.cfg.streams; i++) {
+    cudaStream_t st;
+    const cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      for (auto x : s.streams) cudaStreamDestroy(x);
+      delete srv;
+      return (int)e;
+    }
+    s.streams.push_back(st);
+    s.stream_load.push_back(0);
+  }
+  s.worker = std::thread(worker_main, &s);
+  *out = srv;
+  return 0;
+}
+
+extern "C" glc_status glc_server_submit(glc_server *srv, const glc_serve_request *req, uint64_t *ticket) {
+  if (!srv || !req || !ticket) return fail("serve: null argument");
+  int e = request_check(*req);
+  if (e) return e;
+  Server &s = srv->s;
+  const uint64_t fp = request_footprint(*req);
+  std::lock_guard<std::mutex> lk(s.mu);
+  if (fp > s.cfg.hbm_budget_bytes) {
+    s.rejected++;
+    return fail("serve: request footprint exceeds the HBM budget");
+  }
+  if (s.stop) return fail("serve: server is shutting down");
+  Request q;
+  q.ticket = s.next_ticket++;
+  q.req = *req;
+  q.footprint = fp;
+  q.t_submit = now_s();
+  s.reqs[q.ticket] = q;
+  s.pending.push_back(q.ticket);
+  *ticket = q.ticket;
+  s.cv_work.notify_all();
+  return 0;
+}
+
+extern "C" glc_status glc_server_cancel(glc_server *srv, uint64_t ticket) {
+  if (!srv) return fail("serve: null server");
+  Server &s = srv->s;
+  std::lock_guard<std::mutex> lk(s.mu);
+  auto it = s.reqs.find(ticket);
+  if (it == s.reqs.end()) return fail("serve: unknown ticket");
+  if (it->second.started) return fail("serve: request already started");
+  it->second.cancelled = true;
+  it->second.done = true;
+  it->second.status = (int)cudaErrorInvalidValue;
+  s.cv_done.notify_all();
+  return 0;
+}
+
+extern "C" glc_status glc_server_wait(glc_server *srv, uint64_t ticket, double timeout_s, glc_serve_result *out) {
+  if (!srv || !out) return fail("serve: null argument");
+  Server &s = srv->s;
+  std::unique_lock<std::mutex> lk(s.mu);
+  auto it = s.reqs.find(ticket);
+  if (it == s.reqs.end()) return fail("serve: unknown ticket");
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double>(timeout_s);
+  while (!s.reqs[ticket].done) {
+    if (timeout_s >= 0 && s.cv_done.wait_until(lk, deadline) == std::cv_status::timeout && !s.reqs[ticket].done)
+      return (int)cudaErrorNotReady;
+    if (timeout_s < 0) s.cv_done.wait(lk);
+  }
+  Request &q = s.reqs[ticket];
+  out->ticket = ticket;
+  out->status = q.status;
+  out->queue_s = q.started ? q.t_start - q.t_submit : 0;
+  out->latency_s = q.t_done - q.t_submit;
+  out->device_lde = q.d_lde;
+  out->device_trees = q.d_trees;
+  if (!q.req.keep_resident || q.status) s.reqs.erase(ticket);
+  return 0;
+}
+
+extern "C" glc_status glc_server_release(glc_server *srv, uint64_t ticket) {
+  if (!srv) return fail("serve: null server");
+  Server &s = srv->s;
+  std::lock_guard<std::mutex> lk(s.mu);
+  auto it = s.reqs.find(ticket);
+  if (it == s.reqs.end() || !it->second.done) return fail("serve: no finished resident request with this ticket");
+  Request &q = it->second;
+  cudaStream_t st = s.streams[q.stream >= 0 ? q.stream : 0];
+  if (q.d_lde) cudaFreeAsync(q.d_lde, st);
+  if (q.d_trees) cudaFreeAsync(q.d_trees, st);
+  if (q.req.keep_resident && !q.status) s.used_bytes -= q.footprint;
+  s.reqs.erase(it);
+  s.cv_work.notify_all();
+  return 0;
+}
+
+extern "C" glc_status glc_server_get_stats(glc_server *srv, glc_server_stats *out) {
+  if (!srv || !out) return fail("serve: null argument");
+  Server &s = srv->s;
+  std::lock_guard<std::mutex> lk(s.mu);
+  out->completed = s.completed;
+  out->rejected = s.rejected;
+  out->pending = s.pending.size();
+  out->inflight = s.inflight;
+  out->used_bytes = s.used_bytes;
+  out->peak_bytes = s.peak_bytes;
+  out->peak_inflight = s.peak_inflight;
+  return 0;
+}
+
+extern "C" glc_status glc_server_destroy(glc_server *srv) {
+  if (!srv) return 0;
+  Server &s = srv->s;
+  {
+    std::lock_guard<std::mutex> lk(s.mu);
+    s.stop = true;
+    s.cv_work.notify_all();
+  }
+  if (s.worker.joinable()) s.worker.join();
+  cudaSetDevice(s.device);
+  for (auto &kv : s.reqs) {
+    Request &q = kv.second;
+    if (q.started) {
+      if (q.d_lde) cudaFreeAsync(q.d_lde, s.streams[q.stream]);
+      if (q.d_trees) cudaFreeAsync(q.d_trees, s.streams[q.stream]);
+    }
+  }
+  for (auto st : s.streams) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  delete srv;
+  return 0;
+}

@@ -78,3 +78,12 @@ def random_field_elements(seed, count: int, offset: int = 0) -> np.ndarray:
         ok = alt[alt < np.uint64(P)]
         out[j] = ok[0] if len(ok) else alt[0] % np.uint64(P)
     return out
+
+
+def fill_device(buf, seed, offset: int = 0, stream=None) -> None:
+    """Fills a device buffer with elements offset.. of the stream (glc_fill_random), same values
+    as random_field_elements."""
+    from ._buffers import as_slice, stream_handle
+    from ._lib import call
+    ptr, n = as_slice(buf)
+    call("glc_fill_random", ptr, n, offset, seed_bytes(seed), stream_handle(stream))
