@@ -210,6 +210,10 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     n_ev = 3 + 3 * f
     events = [torch.cuda.Event(enable_timing=True) for _ in range(n_ev)]
+    for e in events:  # torch creates the underlying cudaEvent_t on first record
+        e.record()
+    torch.cuda.synchronize()
+    assert all(e.cuda_event for e in events)
     ev_arr = (C.c_void_p * n_ev)(*[e.cuda_event for e in events])
     jstruct = job._struct()
     lib = glc._lib.lib()
@@ -349,6 +353,177 @@ def run_ours(args, rank, world, local_rank):
     ctx.destroy()
 
 
+# ---------------------------------------------------------------------------------------------
+# Secondary workloads (their own JSON lines; the default run prints the contract line above).
+# ---------------------------------------------------------------------------------------------
+
+def _setup_device(local_rank=0):
+    import torch
+    glc = importlib.import_module("zksync-crypto-gpu_b200")
+    torch.cuda.set_device(local_rank)
+    ctx = glc.Context.create(15, 15)
+    consts = importlib.import_module("zksync-crypto-gpu_b200.p2_constants")
+    rc = consts.env_round_constants()
+    if rc:
+        glc.poseidon2.set_round_constants(rc)
+    tune_path = os.path.join(ROOT, "zksync-crypto-gpu_b200", "tuning_b200.txt")
+    if os.path.exists(tune_path):
+        glc.tuning.load(tune_path)
+    return glc, torch, ctx
+
+
+def uneven_jobs(n_jobs=300, seed=7):
+    """The uneven batch: log2 rows uniform in 12..22, columns in {8,16,32,64,128}, LDE factor 2 or
+    4 (50/50), cap 16; drawn from a seeded generator."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return [(int(rng.integers(12, 23)), int(rng.choice([8, 16, 32, 64, 128])), int(rng.choice([1, 2])), 4)
+            for _ in range(n_jobs)]
+
+
+def run_uneven(args):
+    """Batched (multi-stream + CUDA graph) vs plain one-call-per-job on the uneven batch.  The 300
+    jobs hold ~100 GB of inputs and ~300 GB of outputs, so they run in waves that fit a device
+    budget; every form processes every job."""
+    glc, torch, ctx = _setup_device()
+    syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
+    jobs = uneven_jobs()
+    budget = int(args.budget_gb * (1 << 30))
+    waves, cur, used = [], [], 0
+    for j in sorted(jobs, key=lambda j: -(j[1] << j[0])):
+        sz = glc.CommitJob.sizes(*j)
+        b = 8 * (sz["evals"] + sz["lde"] + sz["trees"] + sz["cap"])
+        if cur and used + b > budget:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(j)
+        used += b
+    waves.append(cur)
+    stream = torch.cuda.current_stream()
+    t = {"plain": 0.0, "batched": 0.0, "graph": 0.0}
+    elements = sum(c << l for l, c, _, _ in jobs)
+    caps_equal = True
+    for wi, wave in enumerate(waves):
+        bufs = []
+        for i, (l, c, e, cap) in enumerate(wave):
+            sz = glc.CommitJob.sizes(l, c, e, cap)
+            dev = lambda k: torch.empty(sz[k], dtype=torch.int64, device="cuda")
+            jb = glc.CommitJob(evals=dev("evals"), log_n=l, cols=c, log_lde=e, log_cap=cap, lde=dev("lde"),
+                               trees=dev("trees"), cap=dev("cap"))
+            syn.fill_device(jb.evals, "uneven-%d-%d" % (wi, i))
+            bufs.append(jb)
+        # warm up every form once (also the graph instantiation), then time one pass of each
+        for jb in bufs:
+            glc.commit.commit(jb)
+        graph = glc.CommitGraph(bufs, n_streams=args.streams)
+        graph.launch()
+        torch.cuda.synchronize()
+        caps_graph = [jb.cap.clone() for jb in bufs]
+        for form in ("plain", "batched", "graph"):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if form == "plain":
+                for jb in bufs:
+                    glc.commit.commit(jb, stream)
+            elif form == "batched":
+                glc.commit.commit_batch(bufs, n_streams=args.streams)
+            else:
+                graph.launch()
+            e1.record()
+            torch.cuda.synchronize()
+            t[form] += e0.elapsed_time(e1)
+        caps_equal &= all(bool((a == jb.cap).all()) for a, jb in zip(caps_graph, bufs))
+        graph.close()
+        del bufs
+        torch.cuda.empty_cache()
+    line = {"workload": "uneven batch: 300 jobs, log2 rows U{12..22}, columns {8..128}, LDE x2/x4, cap 16",
+            "metric": "LDE+Merkle commit elements/s", "unit": "elements/s", "waves": len(waves),
+            "plain": {"ms": t["plain"], "value": elements / (t["plain"] / 1e3)},
+            "batched_streams": {"ms": t["batched"], "value": elements / (t["batched"] / 1e3)},
+            "batched_graph": {"ms": t["graph"], "value": elements / (t["graph"] / 1e3)},
+            "speedup_graph_vs_plain": t["plain"] / t["graph"], "speedup_streams_vs_plain": t["plain"] / t["batched"],
+            "caps_identical_across_forms": caps_equal, "streams": args.streams}
+    print(json.dumps(line), flush=True)
+    ctx.destroy()
+
+
+def run_large(args):
+    """2^22 rows x (128 base + 24 extension) = 176 base columns, LDE x2, cap 16 (~18 GB resident)."""
+    glc, torch, ctx = _setup_device()
+    syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
+    l, c, e, cap = 22, 176, 1, 4
+    sz = glc.CommitJob.sizes(l, c, e, cap)
+    dev = lambda k: torch.empty(sz[k], dtype=torch.int64, device="cuda")
+    jb = glc.CommitJob(evals=dev("evals"), log_n=l, cols=c, log_lde=e, log_cap=cap, lde=dev("lde"),
+                       trees=dev("trees"), cap=dev("cap"))
+    syn.fill_device(jb.evals, "large")
+    for _ in range(args.warmup):
+        glc.commit.commit(jb)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        glc.commit.commit(jb)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    units = job_units(l, c, e, cap)
+    peaks, _ = measured_peaks()
+    lib = glc._lib.lib()
+    blocks, iters = 148 * 32, 2048
+    scratch = torch.empty(blocks * 256, dtype=torch.int64, device="cuda")
+    lib.glc_modmul_probe(scratch.data_ptr(), blocks, 64, None)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    lib.glc_modmul_probe(scratch.data_ptr(), blocks, iters, None)
+    p1.record()
+    torch.cuda.synchronize()
+    mm_peak = blocks * 256 * 8 * iters / (p0.elapsed_time(p1) / 1e3)
+    t_roof = max(units["bytes"] / (peaks["hbm_gbs"] * 1e9), units["modmul"] / mm_peak)
+    print(json.dumps({"workload": "2^22 rows x 176 base columns (128 + 24 extension pairs), LDE x2, cap 16",
+                      "ms_per_step": ms, "value": units["elements"] / (ms / 1e3), "unit": "elements/s",
+                      "hashes_per_s": (units["perms_leaves"] + units["perms_nodes"]) / (ms / 1e3),
+                      "roofline": {"t_roof_ms": t_roof * 1e3, "frac": t_roof * 1e3 / ms, "modmul": units["modmul"],
+                                   "bytes": units["bytes"], "modmul_peak_gs": mm_peak / 1e9,
+                                   "hbm_gbs": peaks["hbm_gbs"]}}), flush=True)
+    ctx.destroy()
+
+
+def run_serve(args):
+    """Poisson arrivals of commitment jobs (log2 rows U[16,23], columns U[8,256], LDE x2/x4) served
+    with continuous batching under an HBM budget; p50/p99 latency, against the plain sequential
+    form (one request on the device at a time).  Host inputs: one pinned buffer of seeded
+    synthetic elements, each request reading its prefix."""
+    import numpy as np
+    glc, torch, ctx = _setup_device()
+    syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
+    rng = np.random.default_rng(11)
+    jobs = [(int(rng.integers(16, 24)), int(rng.integers(8, 257)), int(rng.choice([1, 2])), 4)
+            for _ in range(args.serve_jobs)]
+    max_elems = max(c << l for l, c, _, _ in jobs)
+    d = torch.empty(max_elems, dtype=torch.int64, device="cuda")
+    syn.fill_device(d, "serve")
+    host = torch.empty(max_elems, dtype=torch.int64, pin_memory=True)
+    host.copy_(d)
+    del d
+    torch.cuda.empty_cache()
+    base = host.numpy().view(np.uint64)
+    make = lambda i, l, c: base[:c << l]
+    out = {"workload": "serving: Poisson(%g/s) arrivals, %d jobs, log2 rows U[16,23], columns U[8,256], LDE x2/x4"
+                       % (args.rate, len(jobs)), "budget_gb": args.budget_gb}
+    for name, inflight, streams in (("continuous_batching", args.inflight, args.streams), ("plain_sequential", 1, 1)):
+        with glc.serve.Server(hbm_budget_bytes=int(args.budget_gb * (1 << 30)), max_inflight=inflight,
+                              streams=streams) as srv:
+            r = glc.serve.poisson_load(srv, jobs, rate_per_s=args.rate, seed=3, make_input=make)
+            st = srv.stats()
+        r.pop("caps")
+        r["peak_inflight"] = st["peak_inflight"]
+        r["peak_gb"] = st["peak_bytes"] / (1 << 30)
+        out[name] = r
+    print(json.dumps(out), flush=True)
+    ctx.destroy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -356,7 +531,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-ref-kernels", action="store_true")
+    ap.add_argument("--workload", default="commit", choices=["commit", "uneven", "large", "serve"],
+                    help="commit: the contract line; others print their own JSON")
+    ap.add_argument("--streams", type=int, default=8)
+    ap.add_argument("--budget-gb", type=float, default=120.0)
+    ap.add_argument("--serve-jobs", type=int, default=40)
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--inflight", type=int, default=8)
     args = ap.parse_args()
+    if args.workload != "commit":
+        {"uneven": run_uneven, "large": run_large, "serve": run_serve}[args.workload](args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -23,7 +23,9 @@ def inp(i, log_n, cols):
 
 
 def test_mix_equals_alone(glc, oracle):
-    jobs = [(12, 8, 1, 4), (14, 24, 2, 4), (13, 16, 1, 4), (12, 40, 2, 4), (15, 8, 1, 4), (12, 130, 1, 1)]
+    # the first job runs long enough that the small ones arrive while it is on the device
+    jobs = [(18, 64, 1, 4), (12, 8, 1, 4), (14, 24, 2, 4), (13, 16, 1, 4), (12, 40, 2, 4), (15, 8, 1, 4),
+            (12, 130, 1, 1)]
     with glc.serve.Server(hbm_budget_bytes=8 << 30, max_inflight=4, streams=4) as srv:
         res = glc.serve.poisson_load(srv, jobs, rate_per_s=0, make_input=inp)
         st = srv.stats()

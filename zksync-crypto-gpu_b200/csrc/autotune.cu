@@ -12,18 +12,18 @@
 namespace glc {
 
 static float time_ms(cudaStream_t s, int reps, const std::function<int()> &fn, int *err) {
-  cudaEvent_t a, b;
-  cudaEventCreate(&a);
-  cudaEventCreate(&b);
-  *err = fn();  // warm-up
-  cudaEventRecord(a, s);
-  for (int i = 0; i < reps && !*err; i++) *err = fn();
-  cudaEventRecord(b, s);
-  cudaEventSynchronize(b);
+  cudaEvent_t a = nullptr, b = nullptr;
   float ms = 0;
-  cudaEventElapsedTime(&ms, a, b);
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  *err = (int)cudaEventCreate(&a);
+  if (!*err) *err = (int)cudaEventCreate(&b);
+  if (!*err) *err = fn();  // warm-up
+  if (!*err) *err = (int)cudaEventRecord(a, s);
+  for (int i = 0; i < reps && !*err; i++) *err = fn();
+  if (!*err) *err = (int)cudaEventRecord(b, s);
+  if (!*err) *err = (int)cudaEventSynchronize(b);
+  if (!*err) *err = (int)cudaEventElapsedTime(&ms, a, b);
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
   return reps ? ms / reps : ms;
 }
 
@@ -74,13 +74,21 @@ extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint3
     return fail("autotune: bad size range");
   if (!current_tables()) return fail("autotune: glc_context_create has not been called on this device");
   if (reps == 0) reps = 3;
-  const uint64_t max_elems = (uint64_t)cols << log_n_max;
+  // scratch: the largest NTT batch, and the leaf probe's 128 x 2^17 values (larger than L2, many
+  // column streams, like a real commitment) + 4 x 2^17 digests
+  constexpr uint64_t LEAF_ROWS = 1ull << 17, LEAF_COLS = 128;
+  const uint64_t elems = std::max<uint64_t>((uint64_t)cols << log_n_max, (LEAF_COLS + 4) * LEAF_ROWS);
   uint64_t *buf = nullptr;
-  cudaError_t ce = cudaMalloc(&buf, std::max<uint64_t>(max_elems, 1ull << 22) * sizeof(uint64_t));
+  cudaError_t ce = cudaMalloc(&buf, elems * sizeof(uint64_t));
   if (ce != cudaSuccess) return (int)ce;
-  cudaStream_t s;
-  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-  cudaMemsetAsync(buf, 0x5a, std::max<uint64_t>(max_elems, 1ull << 22) * sizeof(uint64_t), s);
+  cudaStream_t s = nullptr;
+  ce = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(buf, 0x5a, elems * sizeof(uint64_t), s);
+  if (ce != cudaSuccess) {
+    if (s) cudaStreamDestroy(s);
+    cudaFree(buf);
+    return (int)ce;
+  }
   int err = 0;
   for (uint32_t log_n = log_n_min; log_n <= log_n_max && !err; log_n++) {
     const NttTuning saved = ntt_tuning(log_n);
@@ -112,8 +120,8 @@ extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint3
     ntt_tuning(log_n) = err ? saved : best;
   }
   if (!err) {
-    // Poseidon2 leaves: 2^18 rows x 16 columns
-    const uint64_t count = 1ull << 18;
+    // Poseidon2 leaves: LEAF_ROWS rows x LEAF_COLS columns (buf[0, LEAF_COLS * count)), digests after them
+    const uint64_t count = LEAF_ROWS;
     const P2Tuning saved = p2_tuning();
     P2Tuning best = saved;
     float best_ms = 1e30f;
@@ -124,7 +132,7 @@ extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint3
         c.rolled = rolled;
         p2_tuning() = c;
         const float ms = time_ms(s, (int)reps, [&] {
-          return p2_leaves_launch(buf, buf + 16 * count, 0, 16, count, false, false, s);
+          return p2_leaves_launch(buf, buf + LEAF_COLS * count, 0, LEAF_COLS, count, false, false, s);
         }, &err);
         if (err) break;
         if (ms < best_ms) {

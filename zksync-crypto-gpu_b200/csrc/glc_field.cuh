@@ -57,25 +57,25 @@ __device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b) {
   return pack(z0, z1);
 }
 
-// Reduce the 128-bit value hi:lo to [0, 2^64) with carry chains only (ALU pipe):
-//   lo - hh*2^96 == lo - hh;  hl*2^64 == hl*EPS = (hl << 32) - hl;  a carry out is worth EPS.
+// Reduce the 128-bit value hi:lo to [0, 2^64) with carry chains (ALU pipe).  With hi = hh:hl,
+//   V = lo + hl*2^32 - hl - hh  ==  lo + hl*2^64 + hh*2^96  (2^64 == 2^32 - 1, 2^96 == -1),
+// and -2^33 < V < 2^65, so V = c*2^64 + R with c in {-1, 0, 1}; R + c*EPS never wraps again
+// (c = 1 implies R <= 2^64 - 2^33, c = -1 implies R >= 2^64 - 2^33).
 __device__ __forceinline__ uint64_t reduce128(uint64_t lo, uint64_t hi) {
   uint32_t v0, v1;
   asm("{\n\t"
-      ".reg .u32 t0, t1, m, u0, u1, c;\n\t"
-      "sub.cc.u32 t0, %2, %5;\n\t"   // t = lo - hh
-      "subc.cc.u32 t1, %3, 0;\n\t"
-      "subc.u32 m, 0, 0;\n\t"        // m = borrow ? 0xffffffff : 0
-      "sub.cc.u32 t0, t0, m;\n\t"    // borrow: t -= EPS (t >= 2^64 - 2^32 then: no new borrow)
-      "subc.u32 t1, t1, 0;\n\t"
-      "sub.cc.u32 u0, 0, %4;\n\t"    // u = hl * EPS
-      "subc.u32 u1, %4, 0;\n\t"
-      "add.cc.u32 t0, t0, u0;\n\t"   // r = t + u
-      "addc.cc.u32 t1, t1, u1;\n\t"
+      ".reg .u32 t1, c, s0, s1, r0, r1, e0, e1;\n\t"
+      "add.cc.u32 t1, %3, %4;\n\t"   // lo + hl*2^32: 65 bits c:t1:lo0
       "addc.u32 c, 0, 0;\n\t"
-      "neg.s32 c, c;\n\t"
-      "add.cc.u32 %0, t0, c;\n\t"    // carry: r += EPS (r <= 2^64 - 2^33 then: no new carry)
-      "addc.u32 %1, t1, 0;\n\t"
+      "add.cc.u32 s0, %4, %5;\n\t"   // s = hl + hh: 33 bits
+      "addc.u32 s1, 0, 0;\n\t"
+      "sub.cc.u32 r0, %2, s0;\n\t"   // V = (c:t1:lo0) - s
+      "subc.cc.u32 r1, t1, s1;\n\t"
+      "subc.u32 c, c, 0;\n\t"
+      "neg.s32 e0, c;\n\t"           // c*EPS sign-extended to 64 bits
+      "shr.s32 e1, c, 31;\n\t"
+      "add.cc.u32 %0, r0, e0;\n\t"
+      "addc.u32 %1, r1, e1;\n\t"
       "}"
       : "=r"(v0), "=r"(v1)
       : "r"(lo32(lo)), "r"(hi32(lo)), "r"(lo32(hi)), "r"(hi32(hi)));

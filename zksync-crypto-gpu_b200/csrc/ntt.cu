@@ -26,7 +26,8 @@ namespace glc {
 
 static constexpr uint32_t MAX_TILE_LOG = 13;  // 8192 elements = 64 KiB of shared memory
 static constexpr uint32_t PASS_THREADS = 512;
-static constexpr uint32_t SINGLE_PASS_MAX_LOG = 12;  // one column per tile, tile + twiddles <= 64 KiB
+static constexpr uint32_t SINGLE_PASS_MAX_LOG = 12;
+static constexpr int NTT_SMEM_MAX = 140 * 1024;  // tile 64 KiB + twiddles 32 KiB + scaling tables 32 KiB  // one column per tile, tile + twiddles <= 64 KiB
 
 struct PassArgs {
   const uint64_t *in;
@@ -46,7 +47,8 @@ struct PassArgs {
 
 __device__ __forceinline__ uint32_t swz(uint32_t e) { return e ^ ((e >> 4) & 15u); }
 
-__device__ __forceinline__ uint64_t coset_factor(const PassArgs &a, uint32_t j) {
+// s^j (scale 1) or s^-j (scale 2) for the coset shift s = g * w_{2^(L+e)}^c; 1 without extension
+__device__ __forceinline__ uint64_t coset_power(const PassArgs &a, uint32_t j) {
   uint64_t f = 1;
   if (a.log_ext) {
     f = mul(a.g_lo[j & 4095], a.g_hi[j >> 12]);
@@ -57,9 +59,10 @@ __device__ __forceinline__ uint64_t coset_factor(const PassArgs &a, uint32_t j) 
       f = mul(f, mul(a.w_lo[y & 32767], a.w_hi[y >> 15]));
     }
   }
-  if (a.scale == 2) f = mul(f, a.n_inv);
   return f;
 }
+
+__device__ __forceinline__ uint32_t brev_low(uint32_t x, uint32_t bits) { return bits ? __brev(x) >> (32 - bits) : 0; }
 
 template <uint32_t R, bool DIF>
 __device__ __forceinline__ void radix_round(uint64_t *tile, const uint64_t *tws, uint32_t k, uint32_t log_w, uint32_t t) {
@@ -130,6 +133,22 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) ntt_pass_kernel(const PassArg
     const uint32_t m = idx + 1 - (1u << t);
     tws[idx] = a.tw[((uint64_t)hi << t) + m];
   }
+  // Coset / size scaling as two per-CTA tables: the exponent j of element (mid, w) splits as
+  //   natural j = mid * M + (lo0 + w)                      (strided pass, hi = 0)
+  //   bit-reversed j = bitrev_k(mid) << (L - k) + bitrev_{L-k}(hi)  (contiguous pass, W = 1)
+  // so the factor is P[mid] * Q[w] (P carries N^-1 on the inverse side): 2 multiplies per element.
+  uint64_t *Pt = tws + (1u << k);
+  uint64_t *Qt = Pt + (1u << k);
+  if (a.scale) {
+    for (uint32_t m = threadIdx.x; m < (1u << k); m += blockDim.x) {
+      const uint32_t jm = a.j_bitrev ? brev_low(m, k) << (a.log_n - k) : m << log_m;
+      const uint64_t pm = coset_power(a, jm);
+      Pt[m] = a.scale == 2 ? mul(pm, a.n_inv) : pm;
+    }
+    const uint32_t nq = a.j_bitrev ? 1u : (1u << log_w);
+    for (uint32_t w = threadIdx.x; w < nq; w += blockDim.x)
+      Qt[w] = coset_power(a, a.j_bitrev ? brev_low(hi, a.log_n - k) : lo0 + w);
+  }
   const uint32_t col0 = blockIdx.y * a.cols_per_cta;
   const uint32_t col1 = min(col0 + a.cols_per_cta, a.num_cols);
   const uint32_t wmask = (1u << log_w) - 1;
@@ -141,7 +160,7 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) ntt_pass_kernel(const PassArg
     for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
       const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
       uint64_t v = src[i];
-      if (a.scale == 1) v = mul(v, coset_factor(a, a.j_bitrev ? __brev((uint32_t)i) >> (32 - a.log_n) : (uint32_t)i));
+      if (a.scale == 1) v = mul(v, mul(Pt[e >> log_w], Qt[a.j_bitrev ? 0u : (e & wmask)]));
       tile[swz(e)] = v;
     }
     __syncthreads();
@@ -161,7 +180,7 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) ntt_pass_kernel(const PassArg
     for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
       const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
       uint64_t v = tile[swz(e)];
-      if (a.scale == 2) v = mul(v, coset_factor(a, a.j_bitrev ? __brev((uint32_t)i) >> (32 - a.log_n) : (uint32_t)i));
+      if (a.scale == 2) v = mul(v, mul(Pt[e >> log_w], Qt[a.j_bitrev ? 0u : (e & wmask)]));
       dst[i] = canon(v);
     }
   }
@@ -218,9 +237,9 @@ __global__ void __launch_bounds__(256) bitrev_tiled_kernel(const uint64_t *src, 
 }
 
 int ntt_init_device() {
-  cudaError_t e = cudaFuncSetAttribute(ntt_pass_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(ntt_pass_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(ntt_pass_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(ntt_pass_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, NTT_SMEM_MAX);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(ntt_pass_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, NTT_SMEM_MAX);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(ntt_pass_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, NTT_SMEM_MAX);
   return (int)e;
 }
 
@@ -347,7 +366,10 @@ int ntt_launch(const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_n
       uint32_t cpc = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tu.max_cols_per_cta, (tiles_per_col * cols) / want));
       a.cols_per_cta = cpc;
       const uint32_t gy = (cols + cpc - 1) / cpc;
-      const size_t smem = ((size_t(1) << tile_log) + (size_t(1) << ps.k)) * sizeof(uint64_t);
+      // tile + block twiddles (+ the P/Q scaling tables on a scaled pass)
+      const size_t smem = ((size_t(1) << tile_log) + (size_t(1) << ps.k) +
+                           (a.scale ? (size_t(1) << ps.k) + (size_t(1) << ps.log_w) : 0)) *
+                          sizeof(uint64_t);
       const uint32_t threads =
           (uint32_t)std::min<uint64_t>(PASS_THREADS, std::max<uint64_t>(32, (1ull << tile_log) >> tu.radix_bits));
       if (gy > 65535) count_launches((gy - 1) / 65535);

@@ -131,6 +131,36 @@ __device__ __forceinline__ uint64_t w_red(w96 a) {
   return pack(v0, v1);
 }
 
+__device__ __forceinline__ w96 w_shl(w96 a, int k) {  // a * 2^k, k < 32, no overflow of 96 bits
+  w96 r;
+  r.h = __funnelshift_l(a.l1, a.h, k);
+  r.l1 = __funnelshift_l(a.l0, a.l1, k);
+  r.l0 = a.l0 << k;
+  return r;
+}
+// Partial 96 -> 65-bit reduction (h < 2^31): h * 2^64 + l == l + h * EPS = (h * EPS + l0) + l1 * 2^32,
+// kept as a 96-bit value < 2^65 (one mad.wide, one carry add).
+__device__ __forceinline__ w96 w_partial(w96 a) {
+  const uint64_t t = madw(a.h, 0xFFFFFFFFu, (uint64_t)a.l0);
+  w96 r;
+  r.l0 = lo32(t);
+  asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(r.l1), "=r"(r.h) : "r"(hi32(t)), "r"(a.l1));
+  return r;
+}
+
+// The 22 partial rounds with s1..s11 kept partially reduced (< 2^65 in 96 bits) between rounds:
+// only s0 enters the S-box, so only s0 is fully reduced each round.  Bounds per round: the sum
+// of 12 values < 2^69, 2^14 * s_i < 2^79, so every new s_i < 2^80 and its top word < 2^16.
+__device__ __forceinline__ void internal_lazy(uint64_t &s0, w96 t[WIDTH], uint64_t rc0) {
+  constexpr int LOG_MU_MINUS_ONE[WIDTH] = {4, 14, 11, 8, 0, 5, 2, 9, 13, 6, 3, 12};
+  w96 sum = w_add(w_from(s0), t[1]);
+#pragma unroll
+  for (int i = 2; i < WIDTH; i++) sum = w_add(sum, t[i]);
+  s0 = w_red(w_add(w_add(sum, w_shl64(s0, LOG_MU_MINUS_ONE[0])), w_from(rc0)));
+#pragma unroll
+  for (int i = 1; i < WIDTH; i++) t[i] = w_partial(w_add(sum, w_shl(t[i], LOG_MU_MINUS_ONE[i])));
+}
+
 template <int MODE>
 __device__ __forceinline__ void internal_layer(uint64_t s[WIDTH], const uint64_t *rc) {
   constexpr int LOG_MU_MINUS_ONE[WIDTH] = {4, 14, 11, 8, 0, 5, 2, 9, 13, 6, 3, 12};
@@ -160,18 +190,27 @@ __device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
     else
       external_layer<2>(s, c_rc[4]);
   }
-  if (ROLLED) {
-#pragma unroll 1
-    for (int r = 4; r < 25; r++) {
-      s[0] = sbox(s[0]);
-      internal_layer<2>(s, c_rc[r + 1]);
-    }
-  } else {
+  {
+    w96 t[WIDTH];
 #pragma unroll
-    for (int r = 4; r < 25; r++) {
-      s[0] = sbox(s[0]);
-      internal_layer<2>(s, c_rc[r + 1]);
+    for (int i = 1; i < WIDTH; i++) t[i] = w_from(s[i]);
+    uint64_t s0 = s[0];
+    if (ROLLED) {
+#pragma unroll 1
+      for (int r = 4; r < 25; r++) {
+        s0 = sbox(s0);
+        internal_lazy(s0, t, c_rc[r + 1][0]);
+      }
+    } else {
+#pragma unroll
+      for (int r = 4; r < 25; r++) {
+        s0 = sbox(s0);
+        internal_lazy(s0, t, c_rc[r + 1][0]);
+      }
     }
+    s[0] = s0;
+#pragma unroll
+    for (int i = 1; i < WIDTH; i++) s[i] = w_red(t[i]);
   }
   s[0] = sbox(s[0]);
   internal_layer<1>(s, c_rc[26]);
@@ -191,8 +230,9 @@ __device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
 // Leaf hashes (poseidon2_gl_st.cu:25-59): leaf i absorbs values[(i<<r) + row + col*rows*count]
 // column by column, rows within a column, 8 per permutation into state[0..8) (overwrite),
 // zero-padding the last chunk.  Capacity state[8..12) starts at 0 or is loaded from results.
+// at most 80 registers: three 256-thread CTAs (24 warps) per SM
 template <bool ROLLED>
-__global__ void __launch_bounds__(256) p2_leaves_kernel(const uint64_t *values, uint64_t *results, uint32_t log_rows,
+__global__ void __launch_bounds__(256, 3) p2_leaves_kernel(const uint64_t *values, uint64_t *results, uint32_t log_rows,
                                                         uint64_t cols, uint64_t count, bool load_intermediate,
                                                         bool store_intermediate) {
   const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -209,15 +249,18 @@ __global__ void __launch_bounds__(256) p2_leaves_kernel(const uint64_t *values, 
   const uint64_t *v = values + (gid << log_rows);
   const uint64_t col_stride = rows * count;
   if (log_rows == 0) {
-    uint64_t off = 0;
-    for (; off + 8 <= total; off += 8) {
+    // the next chunk's 8 values are loaded before the current permutation runs, so the DRAM
+    // latency of 8 column streams hides behind ~18K instructions of hashing
+    uint64_t nxt[8];
 #pragma unroll
-      for (int i = 0; i < 8; i++) s[i] = __ldcs(v + (off + i) * col_stride);
-      permutation<ROLLED>(s);
-    }
-    if (off < total) {
+    for (int i = 0; i < 8; i++) nxt[i] = (uint64_t)i < total ? __ldcs(v + i * col_stride) : 0;
+    for (uint64_t off = 0; off < total; off += 8) {
 #pragma unroll
-      for (int i = 0; i < 8; i++) s[i] = off + i < total ? __ldcs(v + (off + i) * col_stride) : 0;
+      for (int i = 0; i < 8; i++) s[i] = nxt[i];
+      if (off + 8 < total) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) nxt[i] = off + 8 + i < total ? __ldcs(v + (off + 8 + i) * col_stride) : 0;
+      }
       permutation<ROLLED>(s);
     }
   } else {
@@ -268,13 +311,13 @@ __device__ __forceinline__ void load_children(const uint64_t *layer, uint64_t co
   }
 }
 
-template <bool ALIGNED>
-__global__ void __launch_bounds__(128) p2_nodes_kernel(const uint64_t *values, uint64_t *results, uint64_t count) {
+template <bool ALIGNED, bool ROLLED>
+__global__ void __launch_bounds__(256) p2_nodes_kernel(const uint64_t *values, uint64_t *results, uint64_t count) {
   const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= count) return;
   uint64_t l[4], r[4], o[4];
   load_children<ALIGNED>(values, count, gid, l, r);
-  hash_node(l, r, o);
+  hash_node<ROLLED>(l, r, o);
 #pragma unroll
   for (int k = 0; k < 4; k++) results[k * count + gid] = o[k];
 }
@@ -283,7 +326,7 @@ __global__ void __launch_bounds__(128) p2_nodes_kernel(const uint64_t *values, u
 // produces up to `layers` parent layers, the j-th written to out_j ([4][count >> j] at
 // out + offset of layer j).  out points at the first parent layer; each following layer starts
 // right after the previous one (reference tree layout, poseidon2.rs:276-314).
-template <uint32_t T, bool ALIGNED>
+template <uint32_t T, bool ALIGNED, bool ROLLED>
 __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint64_t *out, uint64_t count,
                                                        uint32_t layers) {
   __shared__ uint64_t sh[4][T];
@@ -298,7 +341,7 @@ __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint6
     const bool live = node < layer_count;
     if (live) {
       load_children<ALIGNED>(in, layer_count, node, l, r);
-      hash_node(l, r, o);
+      hash_node<ROLLED>(l, r, o);
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         dst[k * layer_count + node] = o[k];
@@ -321,7 +364,7 @@ __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint6
         l[k] = sh[k][2 * tid];
         r[k] = sh[k][2 * tid + 1];
       }
-      hash_node(l, r, o);
+      hash_node<ROLLED>(l, r, o);
 #pragma unroll
       for (int k = 0; k < 4; k++) dst[k * layer_count + node] = o[k];
     }
@@ -387,13 +430,19 @@ int p2_leaves_launch(const uint64_t *values, uint64_t *results, uint32_t log_row
 
 int p2_nodes_launch(const uint64_t *values, uint64_t *results, uint64_t count, cudaStream_t stream) {
   if (count == 0) return 0;
-  const uint32_t threads = 128;
+  const P2Tuning &tu = p2_tuning();
+  const uint32_t threads = tu.leaf_threads;
   const uint64_t blocks = (count + threads - 1) / threads;
   if (blocks > 0x7fffffffull) return fail("poseidon2: too many nodes");
-  if ((reinterpret_cast<uintptr_t>(values) & 15) == 0)
-    p2_nodes_kernel<true><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
+  const bool aligned = (reinterpret_cast<uintptr_t>(values) & 15) == 0;
+  if (aligned && tu.rolled)
+    p2_nodes_kernel<true, true><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
+  else if (aligned)
+    p2_nodes_kernel<true, false><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
+  else if (tu.rolled)
+    p2_nodes_kernel<false, true><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
   else
-    p2_nodes_kernel<false><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
+    p2_nodes_kernel<false, false><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
   return last_launch_error();
 }
 
@@ -406,7 +455,7 @@ int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cud
   // Wide layers: one launch per layer keeps every thread busy.  Once a layer no longer fills
   // the GPU a few times over, fused subtree launches cover up to 8 layers each, so the narrow
   // top of the tree costs a handful of launches instead of one per layer.
-  const uint64_t wide = 148ull * 256 * 4;
+  const uint64_t wide = 148ull * 128;
   while (remaining > 0 && count >= wide) {
     const int e = p2_nodes_launch(in, out, count, stream);
     if (e) return e;
@@ -421,10 +470,15 @@ int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cud
     while (l < remaining && (T >> l) >= 1 && l < 8) l++;
     const uint64_t blocks = (count + T - 1) / T;
     if (blocks > 0x7fffffffull) return fail("poseidon2: too many nodes");
-    if ((reinterpret_cast<uintptr_t>(in) & 15) == 0)
-      p2_subtree_kernel<T, true><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
+    const bool aligned = (reinterpret_cast<uintptr_t>(in) & 15) == 0;
+    if (aligned && p2_tuning().rolled)
+      p2_subtree_kernel<T, true, true><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
+    else if (aligned)
+      p2_subtree_kernel<T, true, false><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
+    else if (p2_tuning().rolled)
+      p2_subtree_kernel<T, false, true><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
     else
-      p2_subtree_kernel<T, false><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
+      p2_subtree_kernel<T, false, false><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
     const int e = last_launch_error();
     if (e) return e;
     // advance past the l layers just written
