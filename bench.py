@@ -400,7 +400,15 @@ def run_uneven(args):
         used += b
     waves.append(cur)
     stream = torch.cuda.current_stream()
-    t = {"plain": 0.0, "batched": 0.0, "graph": 0.0}
+    t = {"plain": 0.0, "batched": 0.0, "graph": 0.0, "reference_kernels": 0.0}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import refkern
+        have_ref = refkern.available()
+    except Exception:
+        have_ref = False
+    if have_ref:
+        refkern.call("ref_context_create", 15, 15)
     elements = sum(c << l for l, c, _, _ in jobs)
     caps_equal = True
     for wi, wave in enumerate(waves):
@@ -434,6 +442,35 @@ def run_uneven(args):
             t[form] += e0.elapsed_time(e1)
         caps_equal &= all(bool((a == jb.cap).all()) for a, jb in zip(caps_graph, bufs))
         graph.close()
+        if have_ref:
+            # the reference's own kernels, one call sequence per job (its per-call form)
+            s_ = stream.cuda_stream
+            mono = torch.empty(max(jb.cols << jb.log_n for jb in bufs), dtype=torch.int64, device="cuda")
+
+            def ref_job(jb):
+                n, f = 1 << jb.log_n, 1 << jb.log_lde
+                refkern.call("ref_batch_ntt", jb.evals.data_ptr(), mono.data_ptr(), jb.log_n, jb.cols, n, n, False, True,
+                             0, 0, s_)
+                refkern.call("ref_bit_reverse", mono.data_ptr(), n, mono.data_ptr(), n, jb.log_n, jb.cols, s_)
+                layers = jb.log_n - (jb.log_cap - jb.log_lde) + 1
+                for c in range(f):
+                    coset = int(format(c, "0%db" % jb.log_lde)[::-1], 2)
+                    dst = jb.lde.data_ptr() + c * jb.cols * n * 8
+                    refkern.call("ref_batch_ntt", mono.data_ptr(), dst, jb.log_n, jb.cols, n, n, False, False,
+                                 jb.log_lde, coset, s_)
+                    refkern.call("ref_p2_build_merkle_tree", dst, jb.cols * n, jb.trees.data_ptr() + c * 8 * n * 8,
+                                 8 * n, 0, layers, s_)
+            for jb in bufs[:4]:
+                ref_job(jb)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for jb in bufs:
+                ref_job(jb)
+            e1.record()
+            torch.cuda.synchronize()
+            t["reference_kernels"] += e0.elapsed_time(e1)
+            del mono
         del bufs
         torch.cuda.empty_cache()
     line = {"workload": "uneven batch: 300 jobs, log2 rows U{12..22}, columns {8..128}, LDE x2/x4, cap 16",
@@ -442,6 +479,10 @@ def run_uneven(args):
             "batched_streams": {"ms": t["batched"], "value": elements / (t["batched"] / 1e3)},
             "batched_graph": {"ms": t["graph"], "value": elements / (t["graph"] / 1e3)},
             "speedup_graph_vs_plain": t["plain"] / t["graph"], "speedup_streams_vs_plain": t["plain"] / t["batched"],
+            "reference_kernels_per_call": ({"ms": t["reference_kernels"],
+                                            "value": elements / (t["reference_kernels"] / 1e3),
+                                            "speedup_graph_vs_reference": t["reference_kernels"] / t["graph"]}
+                                           if have_ref else None),
             "caps_identical_across_forms": caps_equal, "streams": args.streams}
     print(json.dumps(line), flush=True)
     ctx.destroy()

@@ -208,8 +208,10 @@ typedef struct glc_ntt_tuning {
   uint32_t l2_chunk_mb;      /* a two-pass NTT runs both passes per chunk of this many MiB */
 } glc_ntt_tuning;
 typedef struct glc_p2_tuning {
-  uint32_t leaf_threads; /* 64, 128 or 256 */
+  uint32_t leaf_threads; /* 64, 128 or 256 (leaf and wide node-layer kernels) */
   uint32_t rolled;       /* 1: partial rounds in a loop, 0: fully unrolled */
+  uint32_t lazy;         /* 1: partial rounds keep 11 of 12 state words partially reduced */
+  uint32_t min_blocks;   /* leaf kernel register cap: 2 -> 128 registers, 3 -> 80 registers */
 } glc_p2_tuning;
 glc_status glc_tuning_get_ntt(uint32_t log_n, glc_ntt_tuning *out);
 glc_status glc_tuning_set_ntt(uint32_t log_n, const glc_ntt_tuning *tuning);

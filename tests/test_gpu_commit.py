@@ -105,18 +105,22 @@ def test_ntt_tuning_invariance(glc, oracle, radix, k1, lw, cpc):
         glc.tuning.set_ntt(log_n, saved.radix_bits, saved.k1, saved.max_log_w, saved.max_cols_per_cta, saved.l2_chunk_mb)
 
 
-@pytest.mark.parametrize("threads,rolled", [(64, 0), (128, 1), (256, 0), (256, 1)])
-def test_leaf_tuning_invariance(glc, oracle, threads, rolled):
+@pytest.mark.parametrize("threads,rolled,lazy,minb", [(64, 0, 0, 2), (128, 1, 1, 3), (256, 0, 1, 2), (256, 1, 0, 3),
+                                                     (128, 0, 0, 3), (256, 1, 1, 2)])
+def test_leaf_tuning_invariance(glc, oracle, threads, rolled, lazy, minb):
     saved = glc.tuning.get_p2()
-    glc.tuning.set_p2(threads, rolled)
+    glc.tuning.set_p2(threads, rolled, lazy, minb)
     try:
         count, cols = 1 << 10, 11
         vals = load_synthetic().random_field_elements("leaf-tune", cols * count)
         d_res = zeros_dev(4 * count)
         glc.GLHasher.compute_leaf_hashes(to_dev(vals), d_res, 0, False, False)
         assert (canon(from_dev(d_res)) == oracle.leaves(vals, 4 * count, 0)).all()
+        d_tree = zeros_dev(8 * count)
+        glc.GLHasher.build_merkle_tree(to_dev(vals), d_tree, 0, None, 11)
+        assert (canon(from_dev(d_tree)) == oracle.build_merkle_tree(vals, 8 * count, 0, 11)).all()
     finally:
-        glc.tuning.set_p2(saved.leaf_threads, saved.rolled)
+        glc.tuning.set_p2(saved.leaf_threads, saved.rolled, saved.lazy, saved.min_blocks)
 
 
 def test_autotune_keeps_results(glc, oracle, tmp_path):

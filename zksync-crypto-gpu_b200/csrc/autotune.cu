@@ -56,16 +56,19 @@ extern "C" glc_status glc_tuning_set_ntt(uint32_t log_n, const glc_ntt_tuning *i
 extern "C" glc_status glc_tuning_get_p2(glc_p2_tuning *out) {
   if (!out) return fail("tuning: bad arguments");
   const P2Tuning &t = p2_tuning();
-  *out = {t.leaf_threads, t.rolled ? 1u : 0u};
+  *out = {t.leaf_threads, t.rolled ? 1u : 0u, t.lazy ? 1u : 0u, t.min_blocks};
   return 0;
 }
 
 extern "C" glc_status glc_tuning_set_p2(const glc_p2_tuning *in) {
   if (!in || (in->leaf_threads != 64 && in->leaf_threads != 128 && in->leaf_threads != 256))
     return fail("tuning: leaf_threads must be 64, 128 or 256");
+  if (in->min_blocks != 2 && in->min_blocks != 3) return fail("tuning: min_blocks must be 2 or 3");
   P2Tuning &t = p2_tuning();
   t.leaf_threads = in->leaf_threads;
   t.rolled = in->rolled != 0;
+  t.lazy = in->lazy != 0;
+  t.min_blocks = in->min_blocks;
   return 0;
 }
 
@@ -74,9 +77,9 @@ extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint3
     return fail("autotune: bad size range");
   if (!current_tables()) return fail("autotune: glc_context_create has not been called on this device");
   if (reps == 0) reps = 3;
-  // scratch: the largest NTT batch, and the leaf probe's 128 x 2^17 values (larger than L2, many
+  // scratch: the largest NTT batch, and the leaf probe's 128 x 2^19 values (larger than L2, many
   // column streams, like a real commitment) + 4 x 2^17 digests
-  constexpr uint64_t LEAF_ROWS = 1ull << 17, LEAF_COLS = 128;
+  constexpr uint64_t LEAF_ROWS = 1ull << 19, LEAF_COLS = 128;
   const uint64_t elems = std::max<uint64_t>((uint64_t)cols << log_n_max, (LEAF_COLS + 4) * LEAF_ROWS);
   uint64_t *buf = nullptr;
   cudaError_t ce = cudaMalloc(&buf, elems * sizeof(uint64_t));
@@ -126,10 +129,14 @@ extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint3
     P2Tuning best = saved;
     float best_ms = 1e30f;
     for (uint32_t th : {128u, 256u})
-      for (bool rolled : {false, true}) {
+      for (bool rolled : {false, true})
+        for (bool lazy : {false, true})
+          for (uint32_t minb : {2u, 3u}) {
         P2Tuning c;
         c.leaf_threads = th;
         c.rolled = rolled;
+        c.lazy = lazy;
+        c.min_blocks = minb;
         p2_tuning() = c;
         const float ms = time_ms(s, (int)reps, [&] {
           return p2_leaves_launch(buf, buf + LEAF_COLS * count, 0, LEAF_COLS, count, false, false, s);
@@ -153,7 +160,7 @@ extern "C" glc_status glc_tuning_save(const char *path) {
   FILE *f = fopen(path, "w");
   if (!f) return fail(std::string("tuning: cannot write ") + path);
   const P2Tuning &p = p2_tuning();
-  fprintf(f, "p2 %u %u\n", p.leaf_threads, p.rolled ? 1u : 0u);
+  fprintf(f, "p2 %u %u %u %u\n", p.leaf_threads, p.rolled ? 1u : 0u, p.lazy ? 1u : 0u, p.min_blocks);
   for (uint32_t l = 1; l <= MAX_LOG_N; l++) {
     const NttTuning &t = ntt_tuning(l);
     fprintf(f, "ntt %u %u %u %u %u %u\n", l, t.radix_bits, t.k1, t.max_log_w, t.max_cols_per_cta, t.l2_chunk_mb);
@@ -171,7 +178,8 @@ extern "C" glc_status glc_tuning_load(const char *path) {
   while (!e && fscanf(f, "%7s", kind) == 1) {
     if (!strcmp(kind, "p2")) {
       glc_p2_tuning p;
-      if (fscanf(f, "%u %u", &p.leaf_threads, &p.rolled) != 2) e = fail("tuning: malformed p2 line");
+      if (fscanf(f, "%u %u %u %u", &p.leaf_threads, &p.rolled, &p.lazy, &p.min_blocks) != 4)
+        e = fail("tuning: malformed p2 line");
       else e = glc_tuning_set_p2(&p);
     } else if (!strcmp(kind, "ntt")) {
       uint32_t l;

@@ -11,6 +11,7 @@
 // NTT passes of one job overlap the integer-bound hashing of another, and the whole batch can
 // be captured into a CUDA graph and replayed (glc_commit_graph_*).
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "glc_field.cuh"
@@ -45,9 +46,39 @@ static uint32_t brev_bits(uint32_t x, uint32_t bits) {
   return r;
 }
 
-int commit_enqueue(const glc_commit_job &j, cudaStream_t stream, cudaEvent_t *events) {
+// Streams that let the cosets of one commitment run side by side: the memory- and ALU-heavy NTT
+// of coset c+1 fills the issue slots the leaf hashing of coset c leaves idle.
+struct CosetStreams {
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> joins;
+  cudaEvent_t fork = nullptr;
+  std::mutex mu;
+};
+static CosetStreams g_coset_streams[MAX_DEVICES];
+
+static int coset_streams_get(uint32_t n, CosetStreams **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= MAX_DEVICES) return fail("commit: device ordinal out of range");
+  CosetStreams &c = g_coset_streams[dev];
+  if (!c.fork && (e = cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming)) != cudaSuccess) return (int)e;
+  while (c.streams.size() < n) {
+    cudaStream_t st;
+    cudaEvent_t ev;
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return (int)e;
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return (int)e;
+    c.streams.push_back(st);
+    c.joins.push_back(ev);
+  }
+  *out = &c;
+  return 0;
+}
+
+int commit_enqueue(const glc_commit_job &j, cudaStream_t stream, cudaEvent_t *events, bool coset_parallel) {
   uint32_t ev = 0;
-  auto mark = [&]() -> int { return events ? (int)cudaEventRecord(events[ev++], stream) : 0; };
+  cudaStream_t cur = stream;
+  auto mark = [&]() -> int { return events ? (int)cudaEventRecord(events[ev++], cur) : 0; };
   const uint64_t n = 1ull << j.log_n;
   const uint32_t f = 1u << j.log_lde;
   const uint64_t coset_elems = n * j.cols;
@@ -62,23 +93,40 @@ int commit_enqueue(const glc_commit_job &j, cudaStream_t stream, cudaEvent_t *ev
   if (e) return e;
   const uint32_t log_ccap = j.log_cap - j.log_lde;
   const uint32_t layers = j.log_n - log_ccap + 1;
+  CosetStreams *cs = nullptr;
+  std::unique_lock<std::mutex> cs_lock;
+  if (coset_parallel && f > 1) {
+    e = coset_streams_get(f - 1, &cs);
+    if (e) return e;
+    cs_lock = std::unique_lock<std::mutex>(cs->mu);
+    if ((e = (int)cudaEventRecord(cs->fork, stream))) return e;
+  }
   for (uint32_t c = 0; c < f; c++) {
+    if (cs && c > 0) {
+      cur = cs->streams[c - 1];
+      if ((e = (int)cudaStreamWaitEvent(cur, cs->fork, 0))) return e;
+    }
     uint64_t *dst = j.lde + (uint64_t)c * coset_elems;
     const uint32_t coset = brev_bits(c, j.log_lde);
-    e = ntt_launch(mono, dst, j.log_n, j.cols, n, n, false, false, j.log_lde, coset, stream, 0);
+    e = ntt_launch(mono, dst, j.log_n, j.cols, n, n, false, false, j.log_lde, coset, cur, 0);
     if (!e) e = mark();
     if (e) return e;
     uint64_t *tree = j.trees + (uint64_t)c * 8 * n;
-    e = p2_leaves_launch(dst, tree, 0, j.cols, n, false, false, stream);
+    e = p2_leaves_launch(dst, tree, 0, j.cols, n, false, false, cur);
     if (!e) e = mark();
     if (e) return e;
     if (layers > 1) {
-      e = p2_tree_nodes_launch(tree, n, layers - 1, stream);
+      e = p2_tree_nodes_launch(tree, n, layers - 1, cur);
       if (e) return e;
     }
     e = mark();
     if (e) return e;
+    if (cs && c > 0) {
+      if ((e = (int)cudaEventRecord(cs->joins[c - 1], cur))) return e;
+      if ((e = (int)cudaStreamWaitEvent(stream, cs->joins[c - 1], 0))) return e;
+    }
   }
+  cur = stream;
   const uint32_t ccap = 1u << log_ccap;
   const uint32_t total = 4 * ccap * f;
   gather_caps_kernel<<<(total + 127) / 128, 128, 0, stream>>>(j.trees, 8 * n, 8 * n - 8ull * ccap, ccap, f, j.cap);
@@ -97,7 +145,7 @@ extern "C" glc_status glc_commit_profiled(const glc_commit_job *job, void *strea
   if (e) return e;
   if (n_events < 3 + 3 * (1u << job->log_lde)) return fail("commit: need 3 + 3 * 2^log_lde events");
   if (!current_tables()) return fail("commit: glc_context_create has not been called on this device");
-  return commit_enqueue(*job, (cudaStream_t)stream, reinterpret_cast<cudaEvent_t *>(events));
+  return commit_enqueue(*job, (cudaStream_t)stream, reinterpret_cast<cudaEvent_t *>(events), true);
 }
 
 extern "C" glc_status glc_commit(const glc_commit_job *job, void *stream) {
@@ -105,5 +153,5 @@ extern "C" glc_status glc_commit(const glc_commit_job *job, void *stream) {
   int e = commit_check(*job);
   if (e) return e;
   if (!current_tables()) return fail("commit: glc_context_create has not been called on this device");
-  return commit_enqueue(*job, (cudaStream_t)stream);
+  return commit_enqueue(*job, (cudaStream_t)stream, nullptr, true);
 }

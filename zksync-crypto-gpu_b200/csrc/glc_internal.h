@@ -61,7 +61,9 @@ NttTuning &ntt_tuning(uint32_t log_n);
 // Launch choices of the Poseidon2 leaf kernel (set by the autotuner, per device).
 struct P2Tuning {
   uint32_t leaf_threads = 256;  // 64, 128 or 256
-  bool rolled = false;          // partial rounds in a loop (smaller code) or fully unrolled
+  bool rolled = true;           // partial rounds in a loop (smaller code) or fully unrolled
+  bool lazy = false;            // partial rounds keep s1..s11 partially reduced
+  uint32_t min_blocks = 2;      // leaf kernel register cap: 2 -> 128 registers, 3 -> 80 registers
 };
 P2Tuning &p2_tuning();
 
@@ -88,6 +90,9 @@ int commit_check(const glc_commit_job &j);
 // Enqueues one job; when `events` is given, records events[0] before the first stage and one
 // event after each stage: monomials, then per coset {NTT, leaves, nodes}, then the cap gather
 // (2 + 3 * 2^log_lde + 1 events).
-int commit_enqueue(const glc_commit_job &j, cudaStream_t stream, cudaEvent_t *events = nullptr);
+// coset_parallel: run the cosets on internal streams forked from `stream` (one call); the batch
+// and serving runtimes pass false because they already spread jobs over streams.
+int commit_enqueue(const glc_commit_job &j, cudaStream_t stream, cudaEvent_t *events = nullptr,
+                   bool coset_parallel = false);
 
 }  // namespace glc

@@ -153,9 +153,11 @@ __device__ __forceinline__ w96 w_partial(w96 a) {
 // of 12 values < 2^69, 2^14 * s_i < 2^79, so every new s_i < 2^80 and its top word < 2^16.
 __device__ __forceinline__ void internal_lazy(uint64_t &s0, w96 t[WIDTH], uint64_t rc0) {
   constexpr int LOG_MU_MINUS_ONE[WIDTH] = {4, 14, 11, 8, 0, 5, 2, 9, 13, 6, 3, 12};
-  w96 sum = w_add(w_from(s0), t[1]);
-#pragma unroll
-  for (int i = 2; i < WIDTH; i++) sum = w_add(sum, t[i]);
+  // t[1..11] do not depend on this round's S-box output: sum them as a tree (depth 4) that runs
+  // beside the S-box, so only one add stands between the S-box and the new state
+  const w96 a = w_add(t[1], t[2]), b = w_add(t[3], t[4]), c = w_add(t[5], t[6]), d = w_add(t[7], t[8]);
+  const w96 e = w_add(w_add(t[9], t[10]), t[11]);
+  const w96 sum = w_add(w_add(w_add(a, b), w_add(c, d)), w_add(e, w_from(s0)));
   s0 = w_red(w_add(w_add(sum, w_shl64(s0, LOG_MU_MINUS_ONE[0])), w_from(rc0)));
 #pragma unroll
   for (int i = 1; i < WIDTH; i++) t[i] = w_partial(w_add(sum, w_shl(t[i], LOG_MU_MINUS_ONE[i])));
@@ -177,8 +179,10 @@ __device__ __forceinline__ void internal_layer(uint64_t s[WIDTH], const uint64_t
 
 // Poseidon2 permutation (poseidon2_gl_st.cu:9-23): M_E, 4 full rounds, 22 partial, 4 full.
 // Round r's constants are added by the linear layer that precedes it.  ROLLED keeps the 22
-// partial rounds in a loop (smaller code, fewer instruction-cache misses); the autotuner picks.
-template <bool ROLLED>
+// partial rounds in a loop (smaller code, fewer instruction-cache misses); LAZY keeps s1..s11
+// partially reduced between partial rounds (fewer instructions, more registers); the autotuner
+// picks per device.
+template <bool ROLLED, bool LAZY>
 __device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
   external_layer<1>(s, c_rc[0]);
 #pragma unroll
@@ -190,7 +194,21 @@ __device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
     else
       external_layer<2>(s, c_rc[4]);
   }
-  {
+  if (!LAZY) {
+    if (ROLLED) {
+#pragma unroll 1
+      for (int r = 4; r < 25; r++) {
+        s[0] = sbox(s[0]);
+        internal_layer<2>(s, c_rc[r + 1]);
+      }
+    } else {
+#pragma unroll
+      for (int r = 4; r < 25; r++) {
+        s[0] = sbox(s[0]);
+        internal_layer<2>(s, c_rc[r + 1]);
+      }
+    }
+  } else {
     w96 t[WIDTH];
 #pragma unroll
     for (int i = 1; i < WIDTH; i++) t[i] = w_from(s[i]);
@@ -230,9 +248,9 @@ __device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
 // Leaf hashes (poseidon2_gl_st.cu:25-59): leaf i absorbs values[(i<<r) + row + col*rows*count]
 // column by column, rows within a column, 8 per permutation into state[0..8) (overwrite),
 // zero-padding the last chunk.  Capacity state[8..12) starts at 0 or is loaded from results.
-// at most 80 registers: three 256-thread CTAs (24 warps) per SM
-template <bool ROLLED>
-__global__ void __launch_bounds__(256, 3) p2_leaves_kernel(const uint64_t *values, uint64_t *results, uint32_t log_rows,
+// MINB = 3 caps registers at 80 (three 256-thread CTAs, 24 warps per SM); MINB = 2 at 128.
+template <bool ROLLED, bool LAZY, int MINB>
+__global__ void __launch_bounds__(256, MINB) p2_leaves_kernel(const uint64_t *values, uint64_t *results, uint32_t log_rows,
                                                         uint64_t cols, uint64_t count, bool load_intermediate,
                                                         bool store_intermediate) {
   const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -261,7 +279,7 @@ __global__ void __launch_bounds__(256, 3) p2_leaves_kernel(const uint64_t *value
 #pragma unroll
         for (int i = 0; i < 8; i++) nxt[i] = off + 8 + i < total ? __ldcs(v + (off + 8 + i) * col_stride) : 0;
       }
-      permutation<ROLLED>(s);
+      permutation<ROLLED, LAZY>(s);
     }
   } else {
     for (uint64_t off = 0; off < total; off += 8) {
@@ -270,7 +288,7 @@ __global__ void __launch_bounds__(256, 3) p2_leaves_kernel(const uint64_t *value
         const uint64_t o = off + i;
         s[i] = o < total ? __ldcs(v + (o & (rows - 1)) + (o >> log_rows) * col_stride) : 0;
       }
-      permutation<ROLLED>(s);
+      permutation<ROLLED, LAZY>(s);
     }
   }
 #pragma unroll
@@ -279,7 +297,7 @@ __global__ void __launch_bounds__(256, 3) p2_leaves_kernel(const uint64_t *value
 
 // Node hashes (poseidon2_gl_st.cu:61-82): node i = P2(L0..L3, R0..R3, 0,0,0,0)[0..4] with
 // L, R = digests 2i and 2i+1 of the [4][2*count] input layer.
-template <bool ROLLED = false>
+template <bool ROLLED, bool LAZY>
 __device__ __forceinline__ void hash_node(const uint64_t l[4], const uint64_t r[4], uint64_t out[4]) {
   uint64_t s[WIDTH];
 #pragma unroll
@@ -288,19 +306,18 @@ __device__ __forceinline__ void hash_node(const uint64_t l[4], const uint64_t r[
     s[4 + k] = r[k];
     s[8 + k] = 0;
   }
-  permutation<ROLLED>(s);
+  permutation<ROLLED, LAZY>(s);
 #pragma unroll
   for (int k = 0; k < 4; k++) out[k] = s[k];
 }
 
 // Children 2i and 2i+1 of row k of a [4][2*count] layer: one 16-byte load when the layer is
 // 16-byte aligned (always, for layers inside a tree buffer), else two 8-byte loads.
-template <bool ALIGNED>
 __device__ __forceinline__ void load_children(const uint64_t *layer, uint64_t count, uint64_t i, uint64_t l[4],
-                                              uint64_t r[4]) {
+                                              uint64_t r[4], bool aligned) {
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    if (ALIGNED) {
+    if (aligned) {
       const ulonglong2 lr = __ldcs(reinterpret_cast<const ulonglong2 *>(layer + k * 2 * count) + i);
       l[k] = lr.x;
       r[k] = lr.y;
@@ -311,13 +328,14 @@ __device__ __forceinline__ void load_children(const uint64_t *layer, uint64_t co
   }
 }
 
-template <bool ALIGNED, bool ROLLED>
-__global__ void __launch_bounds__(256) p2_nodes_kernel(const uint64_t *values, uint64_t *results, uint64_t count) {
+template <bool ROLLED, bool LAZY>
+__global__ void __launch_bounds__(256) p2_nodes_kernel(const uint64_t *values, uint64_t *results, uint64_t count,
+                                                       bool aligned) {
   const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= count) return;
   uint64_t l[4], r[4], o[4];
-  load_children<ALIGNED>(values, count, gid, l, r);
-  hash_node<ROLLED>(l, r, o);
+  load_children(values, count, gid, l, r, aligned);
+  hash_node<ROLLED, LAZY>(l, r, o);
 #pragma unroll
   for (int k = 0; k < 4; k++) results[k * count + gid] = o[k];
 }
@@ -326,9 +344,9 @@ __global__ void __launch_bounds__(256) p2_nodes_kernel(const uint64_t *values, u
 // produces up to `layers` parent layers, the j-th written to out_j ([4][count >> j] at
 // out + offset of layer j).  out points at the first parent layer; each following layer starts
 // right after the previous one (reference tree layout, poseidon2.rs:276-314).
-template <uint32_t T, bool ALIGNED, bool ROLLED>
+template <uint32_t T, bool ROLLED, bool LAZY>
 __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint64_t *out, uint64_t count,
-                                                       uint32_t layers) {
+                                                       uint32_t layers, bool aligned) {
   __shared__ uint64_t sh[4][T];
   const uint32_t tid = threadIdx.x;
   uint64_t layer_count = count;          // nodes in the layer being produced
@@ -340,8 +358,8 @@ __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint6
     uint64_t l[4], r[4], o[4];
     const bool live = node < layer_count;
     if (live) {
-      load_children<ALIGNED>(in, layer_count, node, l, r);
-      hash_node<ROLLED>(l, r, o);
+      load_children(in, layer_count, node, l, r, aligned);
+      hash_node<ROLLED, LAZY>(l, r, o);
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         dst[k * layer_count + node] = o[k];
@@ -364,7 +382,7 @@ __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint6
         l[k] = sh[k][2 * tid];
         r[k] = sh[k][2 * tid + 1];
       }
-      hash_node<ROLLED>(l, r, o);
+      hash_node<ROLLED, LAZY>(l, r, o);
 #pragma unroll
       for (int k = 0; k < 4; k++) dst[k * layer_count + node] = o[k];
     }
@@ -412,6 +430,15 @@ P2Tuning &p2_tuning() {
   return g_p2_tuning[(dev >= 0 && dev < MAX_DEVICES) ? dev : 0];
 }
 
+template <bool ROLLED, bool LAZY>
+static void leaves_go(uint32_t minb, uint32_t blocks, uint32_t threads, cudaStream_t stream, const uint64_t *values,
+                      uint64_t *results, uint32_t log_rows, uint64_t cols, uint64_t count, bool li, bool si) {
+  if (minb >= 3)
+    p2_leaves_kernel<ROLLED, LAZY, 3><<<blocks, threads, 0, stream>>>(values, results, log_rows, cols, count, li, si);
+  else
+    p2_leaves_kernel<ROLLED, LAZY, 2><<<blocks, threads, 0, stream>>>(values, results, log_rows, cols, count, li, si);
+}
+
 int p2_leaves_launch(const uint64_t *values, uint64_t *results, uint32_t log_rows, uint64_t cols, uint64_t count,
                      bool load_intermediate, bool store_intermediate, cudaStream_t stream) {
   if (count == 0) return 0;
@@ -419,12 +446,17 @@ int p2_leaves_launch(const uint64_t *values, uint64_t *results, uint32_t log_row
   const uint32_t threads = tu.leaf_threads;
   const uint64_t blocks = (count + threads - 1) / threads;
   if (blocks > 0x7fffffffull) return fail("poseidon2: too many leaves");
-  if (tu.rolled)
-    p2_leaves_kernel<true><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, log_rows, cols, count,
-                                                                     load_intermediate, store_intermediate);
+#define GLC_LEAVES(R, L) leaves_go<R, L>(tu.min_blocks, (uint32_t)blocks, threads, stream, values, results, log_rows, \
+                                         cols, count, load_intermediate, store_intermediate)
+  if (tu.rolled && tu.lazy)
+    GLC_LEAVES(true, true);
+  else if (tu.rolled)
+    GLC_LEAVES(true, false);
+  else if (tu.lazy)
+    GLC_LEAVES(false, true);
   else
-    p2_leaves_kernel<false><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, log_rows, cols, count,
-                                                                      load_intermediate, store_intermediate);
+    GLC_LEAVES(false, false);
+#undef GLC_LEAVES
   return last_launch_error();
 }
 
@@ -435,14 +467,16 @@ int p2_nodes_launch(const uint64_t *values, uint64_t *results, uint64_t count, c
   const uint64_t blocks = (count + threads - 1) / threads;
   if (blocks > 0x7fffffffull) return fail("poseidon2: too many nodes");
   const bool aligned = (reinterpret_cast<uintptr_t>(values) & 15) == 0;
-  if (aligned && tu.rolled)
-    p2_nodes_kernel<true, true><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
-  else if (aligned)
-    p2_nodes_kernel<true, false><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
+#define GLC_NODES(R, L) p2_nodes_kernel<R, L><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count, aligned)
+  if (tu.rolled && tu.lazy)
+    GLC_NODES(true, true);
   else if (tu.rolled)
-    p2_nodes_kernel<false, true><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
+    GLC_NODES(true, false);
+  else if (tu.lazy)
+    GLC_NODES(false, true);
   else
-    p2_nodes_kernel<false, false><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count);
+    GLC_NODES(false, false);
+#undef GLC_NODES
   return last_launch_error();
 }
 
@@ -471,14 +505,17 @@ int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cud
     const uint64_t blocks = (count + T - 1) / T;
     if (blocks > 0x7fffffffull) return fail("poseidon2: too many nodes");
     const bool aligned = (reinterpret_cast<uintptr_t>(in) & 15) == 0;
-    if (aligned && p2_tuning().rolled)
-      p2_subtree_kernel<T, true, true><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
-    else if (aligned)
-      p2_subtree_kernel<T, true, false><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
-    else if (p2_tuning().rolled)
-      p2_subtree_kernel<T, false, true><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
+    const P2Tuning &tu = p2_tuning();
+#define GLC_SUB(R, L) p2_subtree_kernel<T, R, L><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l, aligned)
+    if (tu.rolled && tu.lazy)
+      GLC_SUB(true, true);
+    else if (tu.rolled)
+      GLC_SUB(true, false);
+    else if (tu.lazy)
+      GLC_SUB(false, true);
     else
-      p2_subtree_kernel<T, false, false><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l);
+      GLC_SUB(false, false);
+#undef GLC_SUB
     const int e = last_launch_error();
     if (e) return e;
     // advance past the l layers just written

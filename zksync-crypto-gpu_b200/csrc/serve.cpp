@@ -43,6 +43,7 @@ struct Server {
   int device = 0;
   std::vector<cudaStream_t> streams;
   std::vector<uint32_t> stream_load;
+  cudaStream_t copy_stream = nullptr;  // result copies to the host
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<uint64_t> pending;
@@ -108,7 +109,8 @@ static int start_request(Server &s, Request &q) {
     j.cap = q.d_cap;
     err = commit_enqueue(j, st);
   }
-  if (!err) err = (int)cudaMemcpyAsync(r.host_cap, q.d_cap, (4ull << r.log_cap) * 8, cudaMemcpyDeviceToHost, st);
+  // the cap goes to the host at completion (worker thread, private copy stream): a copy enqueued
+  // here into pageable memory would block this thread until the whole job had finished
   if (!err) err = (int)cudaEventCreateWithFlags(&q.done_event, cudaEventDisableTiming);
   if (!err) err = (int)cudaEventRecord(q.done_event, st);
   s.stream_load[best]++;
@@ -161,6 +163,12 @@ static void worker_main(Server *s) {
       cudaError_t qe = q.status ? cudaSuccess : cudaEventQuery(q.done_event);
       if (q.status || qe != cudaErrorNotReady) {
         if (!q.status && qe != cudaSuccess) q.status = (int)qe;
+        if (!q.status) {
+          cudaError_t ce = cudaMemcpyAsync(q.req.host_cap, q.d_cap, (4ull << q.req.log_cap) * 8,
+                                           cudaMemcpyDeviceToHost, s->copy_stream);
+          if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->copy_stream);
+          q.status = (int)ce;
+        }
         q.done = true;
         q.t_done = now_s();
         s->stream_load[q.stream]--;
@@ -203,6 +211,10 @@ extern "C" glc_status glc_server_create(const glc_server_config *config, glc_ser
   if (cudaDeviceGetDefaultMemPool(&pool, s.device) == cudaSuccess) {
     uint64_t threshold = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  if (cudaStreamCreateWithFlags(&s.copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete srv;
+    return fail("serve: cannot create the copy stream");
   }
   for (uint32_t i = 0; i < s.cfg.streams; i++) {
     cudaStream_t st;
@@ -332,6 +344,7 @@ extern "C" glc_status glc_server_destroy(glc_server *srv) {
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
   }
+  if (s.copy_stream) cudaStreamDestroy(s.copy_stream);
   delete srv;
   return 0;
 }

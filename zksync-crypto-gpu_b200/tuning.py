@@ -12,7 +12,7 @@ class NttTuning(C.Structure):
 
 
 class P2Tuning(C.Structure):
-    _fields_ = [("leaf_threads", C.c_uint32), ("rolled", C.c_uint32)]
+    _fields_ = [("leaf_threads", C.c_uint32), ("rolled", C.c_uint32), ("lazy", C.c_uint32), ("min_blocks", C.c_uint32)]
 
 
 def get_ntt(log_n: int) -> NttTuning:
@@ -32,8 +32,8 @@ def get_p2() -> P2Tuning:
     return t
 
 
-def set_p2(leaf_threads=256, rolled=0) -> None:
-    t = P2Tuning(leaf_threads, rolled)
+def set_p2(leaf_threads=256, rolled=1, lazy=0, min_blocks=2) -> None:
+    t = P2Tuning(leaf_threads, rolled, lazy, min_blocks)
     call("glc_tuning_set_p2", C.byref(t))
 
 
