@@ -136,9 +136,10 @@ typedef struct glc_commit_job {
 glc_status glc_commit(const glc_commit_job *job, void *stream);
 
 /* glc_commit that also records CUDA events (cudaEvent_t, created by the caller) at the stage
- * boundaries: events[0] before the first stage, then after the monomials, and for each coset
- * after its NTT, its leaf hashes and its node layers, then after the cap gather
- * (n_events >= 3 + 3 * 2^log_lde).  For per-stage timing of a live run. */
+ * boundaries: events[0] before the first stage, events[1] after the monomials, for each coset c
+ * events[2+4c .. 5+4c] at its start, after its NTT, after its leaf hashes and after its node
+ * layers (cosets may run on parallel internal streams), then one after the cap gather
+ * (n_events >= 3 + 4 * 2^log_lde).  For per-stage timing of a live run. */
 glc_status glc_commit_profiled(const glc_commit_job *job, void *stream, void **events, uint32_t n_events);
 
 /* Many commitments as one unit on `stream`: the jobs run concurrently on n_streams internal

@@ -106,6 +106,7 @@ int commit_enqueue(const glc_commit_job &j, cudaStream_t stream, cudaEvent_t *ev
       cur = cs->streams[c - 1];
       if ((e = (int)cudaStreamWaitEvent(cur, cs->fork, 0))) return e;
     }
+    if ((e = mark())) return e;  // coset start (on the stream that runs this coset)
     uint64_t *dst = j.lde + (uint64_t)c * coset_elems;
     const uint32_t coset = brev_bits(c, j.log_lde);
     e = ntt_launch(mono, dst, j.log_n, j.cols, n, n, false, false, j.log_lde, coset, cur, 0);
@@ -143,7 +144,7 @@ extern "C" glc_status glc_commit_profiled(const glc_commit_job *job, void *strea
   if (!job || !events) return fail("commit: null job or events");
   int e = commit_check(*job);
   if (e) return e;
-  if (n_events < 3 + 3 * (1u << job->log_lde)) return fail("commit: need 3 + 3 * 2^log_lde events");
+  if (n_events < 3 + 4 * (1u << job->log_lde)) return fail("commit: need 3 + 4 * 2^log_lde events");
   if (!current_tables()) return fail("commit: glc_context_create has not been called on this device");
   return commit_enqueue(*job, (cudaStream_t)stream, reinterpret_cast<cudaEvent_t *>(events), true);
 }

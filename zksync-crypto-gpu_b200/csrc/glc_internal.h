@@ -87,9 +87,9 @@ int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cud
 int ntt_init_device();  // kernel attributes; called by glc_context_create
 double job_cost(const glc_commit_job &j);
 int commit_check(const glc_commit_job &j);
-// Enqueues one job; when `events` is given, records events[0] before the first stage and one
-// event after each stage: monomials, then per coset {NTT, leaves, nodes}, then the cap gather
-// (2 + 3 * 2^log_lde + 1 events).
+// Enqueues one job; when `events` is given, records events[0] before the first stage, one after
+// the monomials, then per coset {start, after NTT, after leaves, after nodes} on the stream that
+// runs the coset, then one after the cap gather (3 + 4 * 2^log_lde events).
 // coset_parallel: run the cosets on internal streams forked from `stream` (one call); the batch
 // and serving runtimes pass false because they already spread jobs over streams.
 int commit_enqueue(const glc_commit_job &j, cudaStream_t stream, cudaEvent_t *events = nullptr,
