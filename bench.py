@@ -565,6 +565,32 @@ def run_serve(args):
     ctx.destroy()
 
 
+def run_profile_case(args):
+    """A small commitment for profiler captures: 128 columns x 2^log_n rows (default 2^18, 256 MiB of
+    inputs, still larger than L2), LDE x2, cap 16; warm-up plus a few plain glc_commit calls."""
+    glc, torch, ctx = _setup_device()
+    syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
+    l = args.log_n
+    sz = glc.CommitJob.sizes(l, COLS, LOG_LDE, LOG_CAP)
+    dev = lambda k: torch.empty(sz[k], dtype=torch.int64, device="cuda")
+    jb = glc.CommitJob(evals=dev("evals"), log_n=l, cols=COLS, log_lde=LOG_LDE, log_cap=LOG_CAP, lde=dev("lde"),
+                       trees=dev("trees"), cap=dev("cap"))
+    syn.fill_device(jb.evals, "profile")
+    for _ in range(args.warmup):
+        glc.commit.commit(jb)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        glc.commit.commit(jb)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"workload": "profile case: %d columns x 2^%d rows, LDE x2, cap 16" % (COLS, l),
+                      "ms_per_step": ms, "value": (COLS << l) / (ms / 1e3), "unit": "elements/s"}), flush=True)
+    ctx.destroy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -572,8 +598,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-ref-kernels", action="store_true")
-    ap.add_argument("--workload", default="commit", choices=["commit", "uneven", "large", "serve"],
+    ap.add_argument("--workload", default="commit", choices=["commit", "uneven", "large", "serve", "profile"],
                     help="commit: the contract line; others print their own JSON")
+    ap.add_argument("--log-n", type=int, default=18, help="rows of the profile case (log2)")
     ap.add_argument("--streams", type=int, default=8)
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--serve-jobs", type=int, default=40)
@@ -581,7 +608,8 @@ def main():
     ap.add_argument("--inflight", type=int, default=8)
     args = ap.parse_args()
     if args.workload != "commit":
-        {"uneven": run_uneven, "large": run_large, "serve": run_serve}[args.workload](args)
+        {"uneven": run_uneven, "large": run_large, "serve": run_serve,
+         "profile": run_profile_case}[args.workload](args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -44,9 +44,14 @@ def test_commit_plain(glc, oracle, syn, log_n, cols, log_lde, log_cap):
     check_job(oracle, job, ev)
 
 
-def test_commit_without_monomials(glc, oracle, syn):
-    job, ev = make_job(glc, syn, 12, 8, 2, 4, "nomono", keep_monomials=False)
-    glc.commit.commit(job)
+@pytest.mark.parametrize("log_n,cols,log_lde", [(12, 8, 2), (14, 64, 1), (13, 40, 2)])
+def test_commit_without_monomials(glc, oracle, syn, log_n, cols, log_lde):
+    # the monomials then live in the last coset's LDE slot, which that coset transforms in place
+    # while the other cosets (on parallel streams) read them: the sizes are large enough for the
+    # cosets to overlap on the device
+    job, ev = make_job(glc, syn, log_n, cols, log_lde, 4, "nomono-%d-%d" % (log_n, cols), keep_monomials=False)
+    for _ in range(3):
+        glc.commit.commit(job)
     check_job(oracle, job, ev)
 
 

@@ -51,6 +51,7 @@ static uint32_t brev_bits(uint32_t x, uint32_t bits) {
 struct CosetStreams {
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> joins;
+  std::vector<cudaEvent_t> ntt_done;  // coset c's NTT has read the monomials (c < f - 1)
   cudaEvent_t fork = nullptr;
   std::mutex mu;
 };
@@ -65,11 +66,13 @@ static int coset_streams_get(uint32_t n, CosetStreams **out) {
   if (!c.fork && (e = cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming)) != cudaSuccess) return (int)e;
   while (c.streams.size() < n) {
     cudaStream_t st;
-    cudaEvent_t ev;
+    cudaEvent_t ev, nd;
     if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return (int)e;
     if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return (int)e;
+    if ((e = cudaEventCreateWithFlags(&nd, cudaEventDisableTiming)) != cudaSuccess) return (int)e;
     c.streams.push_back(st);
     c.joins.push_back(ev);
+    c.ntt_done.push_back(nd);
   }
   *out = &c;
   return 0;
@@ -109,7 +112,14 @@ int commit_enqueue(const glc_commit_job &j, cudaStream_t stream, cudaEvent_t *ev
     if ((e = mark())) return e;  // coset start (on the stream that runs this coset)
     uint64_t *dst = j.lde + (uint64_t)c * coset_elems;
     const uint32_t coset = brev_bits(c, j.log_lde);
+    // Without a monomials buffer the last coset transforms the monomials in place: on parallel
+    // streams it must wait until every other coset's NTT has read them.
+    const bool mono_in_lde = !j.monomials;
+    if (cs && mono_in_lde && c == f - 1)
+      for (uint32_t d = 0; d + 1 < f; d++)
+        if ((e = (int)cudaStreamWaitEvent(cur, cs->ntt_done[d], 0))) return e;
     e = ntt_launch(mono, dst, j.log_n, j.cols, n, n, false, false, j.log_lde, coset, cur, 0);
+    if (!e && cs && mono_in_lde && c + 1 < f) e = (int)cudaEventRecord(cs->ntt_done[c], cur);
     if (!e) e = mark();
     if (e) return e;
     uint64_t *tree = j.trees + (uint64_t)c * 8 * n;
