@@ -142,6 +142,19 @@ glc_status glc_commit(const glc_commit_job *job, void *stream);
  * (n_events >= 3 + 4 * 2^log_lde).  For per-stage timing of a live run. */
 glc_status glc_commit_profiled(const glc_commit_job *job, void *stream, void **events, uint32_t n_events);
 
+/* The cap of one commitment, computed without allocating any device memory (no counterpart in
+ * the reference).  For callers that cannot call cudaMalloc: a device allocator or allocation
+ * callback that needs a commitment while serving an allocation, a plugin whose host framework
+ * owns all device memory, a process whose memory another framework has already reserved.  The
+ * LDE cosets and subtrees live in one 2^24-element (128 MiB) array compiled into the library,
+ * held by every GPU that loads it: jobs with 2^log_lde * (cols + 8) * 2^log_n > 2^24 are rejected.
+ * evals, stride, sizes and cap ([4][2^log_cap], device) mean what they mean in glc_commit_job.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress), so make
+ * it before any stream capture on that device.  Calls share the array: calls that overlap on the
+ * GPU race; calls ordered on one stream or by events do not.  Needs glc_context_create. */
+glc_status glc_commit_cap_noalloc(const uint64_t *evals, uint64_t evals_stride, uint32_t log_n, uint32_t cols,
+                                  uint32_t log_lde, uint32_t log_cap, uint64_t *cap, void *stream);
+
 /* Many commitments as one unit on `stream`: the jobs run concurrently on n_streams internal
  * streams (0 = 8), largest first, balanced by estimated cost; `stream` waits for all of them.
  * Capturable into a CUDA graph. */

@@ -49,6 +49,7 @@ SIGNATURES = {
     "glc_poseidon2_gather_merkle_paths": (C.c_int, [u32p, sz, u64p, sz, u64p, sz, u32, vp]),
     "glc_commit": (C.c_int, [vp, vp]),
     "glc_commit_profiled": (C.c_int, [vp, vp, vp, u32]),
+    "glc_commit_cap_noalloc": (C.c_int, [u64p, u64, u32, u32, u32, u32, u64p, vp]),
     "glc_launch_count": (C.c_uint64, []),
     "glc_commit_batch": (C.c_int, [vp, u32, u32, vp]),
     "glc_commit_graph_create": (C.c_int, [vp, u32, u32, vp]),
