@@ -223,7 +223,7 @@ typedef struct glc_ntt_tuning {
 } glc_ntt_tuning;
 typedef struct glc_p2_tuning {
   uint32_t leaf_threads; /* 64, 128 or 256 (leaf and wide node-layer kernels) */
-  uint32_t rolled;       /* 1: partial rounds in a loop, 0: fully unrolled */
+  uint32_t rolled;       /* 0: fully unrolled, 1: partial rounds in a loop, 2: full rounds too */
   uint32_t lazy;         /* 1: partial rounds keep 11 of 12 state words partially reduced */
   uint32_t min_blocks;   /* leaf kernel register cap: 2 -> 128 registers, 3 -> 80 registers */
 } glc_p2_tuning;

@@ -1,6 +1,6 @@
 // Autotuner: per device, times candidate launch configurations of the NTT (radix bits per
 // register round, stages in the strided pass, tile width, columns per CTA, L2 chunk size) for
-// each size, and of the Poseidon2 leaf kernel (threads per CTA, rolled or unrolled partial
+// each size, and of the Poseidon2 leaf kernel (threads per CTA, unrolled / partly / fully rolled
 // rounds), installs the fastest, and saves / loads the table as text.
 #include <cstdio>
 #include <cstring>
@@ -56,7 +56,7 @@ extern "C" glc_status glc_tuning_set_ntt(uint32_t log_n, const glc_ntt_tuning *i
 extern "C" glc_status glc_tuning_get_p2(glc_p2_tuning *out) {
   if (!out) return fail("tuning: bad arguments");
   const P2Tuning &t = p2_tuning();
-  *out = {t.leaf_threads, t.rolled ? 1u : 0u, t.lazy ? 1u : 0u, t.min_blocks};
+  *out = {t.leaf_threads, t.rolled, t.lazy ? 1u : 0u, t.min_blocks};
   return 0;
 }
 
@@ -64,9 +64,10 @@ extern "C" glc_status glc_tuning_set_p2(const glc_p2_tuning *in) {
   if (!in || (in->leaf_threads != 64 && in->leaf_threads != 128 && in->leaf_threads != 256))
     return fail("tuning: leaf_threads must be 64, 128 or 256");
   if (in->min_blocks != 2 && in->min_blocks != 3) return fail("tuning: min_blocks must be 2 or 3");
+  if (in->rolled > 2) return fail("tuning: rolled must be 0, 1 or 2");
   P2Tuning &t = p2_tuning();
   t.leaf_threads = in->leaf_threads;
-  t.rolled = in->rolled != 0;
+  t.rolled = in->rolled;
   t.lazy = in->lazy != 0;
   t.min_blocks = in->min_blocks;
   return 0;
@@ -129,7 +130,7 @@ extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint3
     P2Tuning best = saved;
     float best_ms = 1e30f;
     for (uint32_t th : {128u, 256u})
-      for (bool rolled : {false, true})
+      for (uint32_t rolled : {0u, 1u, 2u})
         for (bool lazy : {false, true})
           for (uint32_t minb : {2u, 3u}) {
         P2Tuning c;
@@ -160,7 +161,7 @@ extern "C" glc_status glc_tuning_save(const char *path) {
   FILE *f = fopen(path, "w");
   if (!f) return fail(std::string("tuning: cannot write ") + path);
   const P2Tuning &p = p2_tuning();
-  fprintf(f, "p2 %u %u %u %u\n", p.leaf_threads, p.rolled ? 1u : 0u, p.lazy ? 1u : 0u, p.min_blocks);
+  fprintf(f, "p2 %u %u %u %u\n", p.leaf_threads, p.rolled, p.lazy ? 1u : 0u, p.min_blocks);
   for (uint32_t l = 1; l <= MAX_LOG_N; l++) {
     const NttTuning &t = ntt_tuning(l);
     fprintf(f, "ntt %u %u %u %u %u %u\n", l, t.radix_bits, t.k1, t.max_log_w, t.max_cols_per_cta, t.l2_chunk_mb);

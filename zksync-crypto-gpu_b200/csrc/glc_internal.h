@@ -60,9 +60,9 @@ NttTuning &ntt_tuning(uint32_t log_n);
 
 // Launch choices of the Poseidon2 leaf kernel (set by the autotuner, per device).
 struct P2Tuning {
-  uint32_t leaf_threads = 256;  // 64, 128 or 256
-  bool rolled = true;           // partial rounds in a loop (smaller code) or fully unrolled
-  bool lazy = false;            // partial rounds keep s1..s11 partially reduced
+  uint32_t leaf_threads = 128;  // 64, 128 or 256
+  uint32_t rolled = 2;          // 0: every round unrolled; 1: partial rounds in a loop; 2: all rounds in loops
+  bool lazy = true;             // partial rounds keep s1..s11 partially reduced
   uint32_t min_blocks = 2;      // leaf kernel register cap: 2 -> 128 registers, 3 -> 80 registers
 };
 P2Tuning &p2_tuning();

@@ -90,6 +90,15 @@ __device__ __forceinline__ void external_layer(uint64_t s[WIDTH], const uint64_t
   }
 }
 
+// M_E with constants chosen at run time (one copy of the code for every full round): element 0
+// adds rc[0] & m0, elements 1..11 add rc[i] & m.
+__device__ __forceinline__ void external_layer_masked(uint64_t s[WIDTH], const uint64_t *rc, uint64_t m0, uint64_t m) {
+  uint64_t k[WIDTH];
+#pragma unroll
+  for (int i = 0; i < WIDTH; i++) k[i] = rc[i] & (i == 0 ? m0 : m);
+  external_layer<1>(s, k);
+}
+
 // ---- M_I = J + diag(2^LOG_MU_MINUS_ONE) (poseidon2_gl_st.cuh:57-65) ----
 // 96-bit lazy sums with carry chains (ALU pipe: the S-box products already load the IMAD pipe),
 // one 96 -> 64 fold per element.
@@ -177,23 +186,9 @@ __device__ __forceinline__ void internal_layer(uint64_t s[WIDTH], const uint64_t
   }
 }
 
-// Poseidon2 permutation (poseidon2_gl_st.cu:9-23): M_E, 4 full rounds, 22 partial, 4 full.
-// Round r's constants are added by the linear layer that precedes it.  ROLLED keeps the 22
-// partial rounds in a loop (smaller code, fewer instruction-cache misses); LAZY keeps s1..s11
-// partially reduced between partial rounds (fewer instructions, more registers); the autotuner
-// picks per device.
+// The 22 partial rounds plus the last one's internal layer, which adds round 26's constants.
 template <bool ROLLED, bool LAZY>
-__device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
-  external_layer<1>(s, c_rc[0]);
-#pragma unroll
-  for (int r = 0; r < 4; r++) {
-#pragma unroll
-    for (int i = 0; i < WIDTH; i++) s[i] = sbox(s[i]);
-    if (r < 3)
-      external_layer<1>(s, c_rc[r + 1]);
-    else
-      external_layer<2>(s, c_rc[4]);
-  }
+__device__ __forceinline__ void partial_rounds(uint64_t s[WIDTH]) {
   if (!LAZY) {
     if (ROLLED) {
 #pragma unroll 1
@@ -232,14 +227,48 @@ __device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
   }
   s[0] = sbox(s[0]);
   internal_layer<1>(s, c_rc[26]);
+}
+
+// Poseidon2 permutation (poseidon2_gl_st.cu:9-23): M_E, 4 full rounds, 22 partial, 4 full.
+// Round r's constants are added by the linear layer that precedes it.  ROLL = 0 unrolls every
+// round; ROLL = 1 keeps the 22 partial rounds in a loop; ROLL = 2 also runs the 8 full rounds
+// through one loop body (about a quarter of the code: the unrolled permutation is larger than
+// the instruction cache, and warps at different rounds evict each other's code).  LAZY keeps
+// s1..s11 partially reduced between partial rounds.  The autotuner picks per device.
+template <int ROLL, bool LAZY>
+__device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
+  external_layer<1>(s, c_rc[0]);
+  if (ROLL == 2) {
+#pragma unroll 1
+    for (int q = 0; q < 8; q++) {
 #pragma unroll
-  for (int r = 26; r < 30; r++) {
+      for (int i = 0; i < WIDTH; i++) s[i] = sbox(s[i]);
+      // full round r = q (q < 4) or q + 22; the layer after it adds round r + 1's constants:
+      // all of them, only element 0's before the partial rounds (q == 3), none after the last
+      const int r = q < 4 ? q : q + 22;
+      external_layer_masked(s, c_rc[q == 7 ? 0 : r + 1], q == 7 ? 0ull : ~0ull, (q == 3 || q == 7) ? 0ull : ~0ull);
+      if (q == 3) partial_rounds<true, LAZY>(s);
+    }
+  } else {
 #pragma unroll
-    for (int i = 0; i < WIDTH; i++) s[i] = sbox(s[i]);
-    if (r < 29)
-      external_layer<1>(s, c_rc[r + 1]);
-    else
-      external_layer<0>(s, nullptr);
+    for (int r = 0; r < 4; r++) {
+#pragma unroll
+      for (int i = 0; i < WIDTH; i++) s[i] = sbox(s[i]);
+      if (r < 3)
+        external_layer<1>(s, c_rc[r + 1]);
+      else
+        external_layer<2>(s, c_rc[4]);
+    }
+    partial_rounds<ROLL == 1, LAZY>(s);
+#pragma unroll
+    for (int r = 26; r < 30; r++) {
+#pragma unroll
+      for (int i = 0; i < WIDTH; i++) s[i] = sbox(s[i]);
+      if (r < 29)
+        external_layer<1>(s, c_rc[r + 1]);
+      else
+        external_layer<0>(s, nullptr);
+    }
   }
 #pragma unroll
   for (int i = 0; i < WIDTH; i++) s[i] = canon(s[i]);
@@ -249,7 +278,7 @@ __device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
 // column by column, rows within a column, 8 per permutation into state[0..8) (overwrite),
 // zero-padding the last chunk.  Capacity state[8..12) starts at 0 or is loaded from results.
 // MINB = 3 caps registers at 80 (three 256-thread CTAs, 24 warps per SM); MINB = 2 at 128.
-template <bool ROLLED, bool LAZY, int MINB>
+template <int ROLL, bool LAZY, int MINB>
 __global__ void __launch_bounds__(256, MINB) p2_leaves_kernel(const uint64_t *values, uint64_t *results, uint32_t log_rows,
                                                         uint64_t cols, uint64_t count, bool load_intermediate,
                                                         bool store_intermediate) {
@@ -266,30 +295,24 @@ __global__ void __launch_bounds__(256, MINB) p2_leaves_kernel(const uint64_t *va
   const uint64_t total = rows * cols;
   const uint64_t *v = values + (gid << log_rows);
   const uint64_t col_stride = rows * count;
-  if (log_rows == 0) {
-    // the next chunk's 8 values are loaded before the current permutation runs, so the DRAM
-    // latency of 8 column streams hides behind ~18K instructions of hashing
-    uint64_t nxt[8];
+  // value o of this leaf: row o % rows of column o / rows.  The next chunk's 8 values are loaded
+  // before the current permutation runs, so the DRAM latency of 8 column streams hides behind
+  // ~15K instructions of hashing.  One permutation call site keeps the code small.
+  uint64_t nxt[8];
 #pragma unroll
-    for (int i = 0; i < 8; i++) nxt[i] = (uint64_t)i < total ? __ldcs(v + i * col_stride) : 0;
-    for (uint64_t off = 0; off < total; off += 8) {
+  for (int i = 0; i < 8; i++)
+    nxt[i] = (uint64_t)i < total ? __ldcs(v + ((uint64_t)i & (rows - 1)) + ((uint64_t)i >> log_rows) * col_stride) : 0;
+  for (uint64_t off = 0; off < total; off += 8) {
 #pragma unroll
-      for (int i = 0; i < 8; i++) s[i] = nxt[i];
-      if (off + 8 < total) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) nxt[i] = off + 8 + i < total ? __ldcs(v + (off + 8 + i) * col_stride) : 0;
-      }
-      permutation<ROLLED, LAZY>(s);
-    }
-  } else {
-    for (uint64_t off = 0; off < total; off += 8) {
+    for (int i = 0; i < 8; i++) s[i] = nxt[i];
+    if (off + 8 < total) {
 #pragma unroll
       for (int i = 0; i < 8; i++) {
-        const uint64_t o = off + i;
-        s[i] = o < total ? __ldcs(v + (o & (rows - 1)) + (o >> log_rows) * col_stride) : 0;
+        const uint64_t o = off + 8 + i;
+        nxt[i] = o < total ? __ldcs(v + (o & (rows - 1)) + (o >> log_rows) * col_stride) : 0;
       }
-      permutation<ROLLED, LAZY>(s);
     }
+    permutation<ROLL, LAZY>(s);
   }
 #pragma unroll
   for (int k = 0; k < 4; k++) results[gid + k * count] = canon(store_intermediate ? s[8 + k] : s[k]);
@@ -297,7 +320,7 @@ __global__ void __launch_bounds__(256, MINB) p2_leaves_kernel(const uint64_t *va
 
 // Node hashes (poseidon2_gl_st.cu:61-82): node i = P2(L0..L3, R0..R3, 0,0,0,0)[0..4] with
 // L, R = digests 2i and 2i+1 of the [4][2*count] input layer.
-template <bool ROLLED, bool LAZY>
+template <int ROLL, bool LAZY>
 __device__ __forceinline__ void hash_node(const uint64_t l[4], const uint64_t r[4], uint64_t out[4]) {
   uint64_t s[WIDTH];
 #pragma unroll
@@ -306,7 +329,7 @@ __device__ __forceinline__ void hash_node(const uint64_t l[4], const uint64_t r[
     s[4 + k] = r[k];
     s[8 + k] = 0;
   }
-  permutation<ROLLED, LAZY>(s);
+  permutation<ROLL, LAZY>(s);
 #pragma unroll
   for (int k = 0; k < 4; k++) out[k] = s[k];
 }
@@ -328,14 +351,14 @@ __device__ __forceinline__ void load_children(const uint64_t *layer, uint64_t co
   }
 }
 
-template <bool ROLLED, bool LAZY>
+template <int ROLL, bool LAZY>
 __global__ void __launch_bounds__(256) p2_nodes_kernel(const uint64_t *values, uint64_t *results, uint64_t count,
                                                        bool aligned) {
   const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= count) return;
   uint64_t l[4], r[4], o[4];
   load_children(values, count, gid, l, r, aligned);
-  hash_node<ROLLED, LAZY>(l, r, o);
+  hash_node<ROLL, LAZY>(l, r, o);
 #pragma unroll
   for (int k = 0; k < 4; k++) results[k * count + gid] = o[k];
 }
@@ -344,7 +367,7 @@ __global__ void __launch_bounds__(256) p2_nodes_kernel(const uint64_t *values, u
 // produces up to `layers` parent layers, the j-th written to out_j ([4][count >> j] at
 // out + offset of layer j).  out points at the first parent layer; each following layer starts
 // right after the previous one (reference tree layout, poseidon2.rs:276-314).
-template <uint32_t T, bool ROLLED, bool LAZY>
+template <uint32_t T, int ROLL, bool LAZY>
 __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint64_t *out, uint64_t count,
                                                        uint32_t layers, bool aligned) {
   __shared__ uint64_t sh[4][T];
@@ -359,7 +382,7 @@ __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint6
     const bool live = node < layer_count;
     if (live) {
       load_children(in, layer_count, node, l, r, aligned);
-      hash_node<ROLLED, LAZY>(l, r, o);
+      hash_node<ROLL, LAZY>(l, r, o);
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         dst[k * layer_count + node] = o[k];
@@ -382,7 +405,7 @@ __global__ void __launch_bounds__(T) p2_subtree_kernel(const uint64_t *in, uint6
         l[k] = sh[k][2 * tid];
         r[k] = sh[k][2 * tid + 1];
       }
-      hash_node<ROLLED, LAZY>(l, r, o);
+      hash_node<ROLL, LAZY>(l, r, o);
 #pragma unroll
       for (int k = 0; k < 4; k++) dst[k * layer_count + node] = o[k];
     }
@@ -430,14 +453,31 @@ P2Tuning &p2_tuning() {
   return g_p2_tuning[(dev >= 0 && dev < MAX_DEVICES) ? dev : 0];
 }
 
-template <bool ROLLED, bool LAZY>
+template <int ROLL, bool LAZY>
 static void leaves_go(uint32_t minb, uint32_t blocks, uint32_t threads, cudaStream_t stream, const uint64_t *values,
                       uint64_t *results, uint32_t log_rows, uint64_t cols, uint64_t count, bool li, bool si) {
   if (minb >= 3)
-    p2_leaves_kernel<ROLLED, LAZY, 3><<<blocks, threads, 0, stream>>>(values, results, log_rows, cols, count, li, si);
+    p2_leaves_kernel<ROLL, LAZY, 3><<<blocks, threads, 0, stream>>>(values, results, log_rows, cols, count, li, si);
   else
-    p2_leaves_kernel<ROLLED, LAZY, 2><<<blocks, threads, 0, stream>>>(values, results, log_rows, cols, count, li, si);
+    p2_leaves_kernel<ROLL, LAZY, 2><<<blocks, threads, 0, stream>>>(values, results, log_rows, cols, count, li, si);
 }
+
+// Calls F<ROLL, LAZY>() for the tuned variant.
+#define GLC_P2_VARIANT(tu, F)             \
+  do {                                    \
+    if ((tu).rolled >= 2 && (tu).lazy)    \
+      F(2, true);                         \
+    else if ((tu).rolled >= 2)            \
+      F(2, false);                        \
+    else if ((tu).rolled && (tu).lazy)    \
+      F(1, true);                         \
+    else if ((tu).rolled)                 \
+      F(1, false);                        \
+    else if ((tu).lazy)                   \
+      F(0, true);                         \
+    else                                  \
+      F(0, false);                        \
+  } while (0)
 
 int p2_leaves_launch(const uint64_t *values, uint64_t *results, uint32_t log_rows, uint64_t cols, uint64_t count,
                      bool load_intermediate, bool store_intermediate, cudaStream_t stream) {
@@ -448,14 +488,7 @@ int p2_leaves_launch(const uint64_t *values, uint64_t *results, uint32_t log_row
   if (blocks > 0x7fffffffull) return fail("poseidon2: too many leaves");
 #define GLC_LEAVES(R, L) leaves_go<R, L>(tu.min_blocks, (uint32_t)blocks, threads, stream, values, results, log_rows, \
                                          cols, count, load_intermediate, store_intermediate)
-  if (tu.rolled && tu.lazy)
-    GLC_LEAVES(true, true);
-  else if (tu.rolled)
-    GLC_LEAVES(true, false);
-  else if (tu.lazy)
-    GLC_LEAVES(false, true);
-  else
-    GLC_LEAVES(false, false);
+  GLC_P2_VARIANT(tu, GLC_LEAVES);
 #undef GLC_LEAVES
   return last_launch_error();
 }
@@ -468,14 +501,7 @@ int p2_nodes_launch(const uint64_t *values, uint64_t *results, uint64_t count, c
   if (blocks > 0x7fffffffull) return fail("poseidon2: too many nodes");
   const bool aligned = (reinterpret_cast<uintptr_t>(values) & 15) == 0;
 #define GLC_NODES(R, L) p2_nodes_kernel<R, L><<<(uint32_t)blocks, threads, 0, stream>>>(values, results, count, aligned)
-  if (tu.rolled && tu.lazy)
-    GLC_NODES(true, true);
-  else if (tu.rolled)
-    GLC_NODES(true, false);
-  else if (tu.lazy)
-    GLC_NODES(false, true);
-  else
-    GLC_NODES(false, false);
+  GLC_P2_VARIANT(tu, GLC_NODES);
 #undef GLC_NODES
   return last_launch_error();
 }
@@ -507,14 +533,7 @@ int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cud
     const bool aligned = (reinterpret_cast<uintptr_t>(in) & 15) == 0;
     const P2Tuning &tu = p2_tuning();
 #define GLC_SUB(R, L) p2_subtree_kernel<T, R, L><<<(uint32_t)blocks, T, 0, stream>>>(in, out, count, l, aligned)
-    if (tu.rolled && tu.lazy)
-      GLC_SUB(true, true);
-    else if (tu.rolled)
-      GLC_SUB(true, false);
-    else if (tu.lazy)
-      GLC_SUB(false, true);
-    else
-      GLC_SUB(false, false);
+    GLC_P2_VARIANT(tu, GLC_SUB);
 #undef GLC_SUB
     const int e = last_launch_error();
     if (e) return e;
