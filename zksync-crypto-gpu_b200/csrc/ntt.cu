@@ -38,6 +38,8 @@ struct PassArgs {
   uint32_t dif;  // 0: n2b stages (DIT, increasing), 1: b2n stages (DIF, decreasing)
   const uint64_t *tw;
   uint32_t scale;     // 0: none, 1: x s^j on load, 2: x N^-1 s^-j on store
+  uint32_t fold;      // 1: forward n2b coset NTT with s folded into the block twiddles
+  uint32_t last;      // last pass: canonical output
   uint32_t j_bitrev;  // exponent j = bitrev_L(position) instead of position
   uint32_t log_ext, coset;
   uint64_t n_inv;
@@ -127,11 +129,20 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) ntt_pass_kernel(const PassArg
   const uint32_t hi = blockIdx.x >> log_tph;
   const uint32_t lo0 = (blockIdx.x & ((1u << log_tph) - 1)) << log_w;
   const uint64_t base_i = ((uint64_t)hi << (a.log_n - a.s0)) + lo0;
-  // tws[2^t - 1 + m] = T[hi * 2^t + m]: block twiddles of stage s0 + t for this hi
+  // tws[2^t - 1 + m] = T[hi * 2^t + m]: block twiddles of stage s0 + t for this hi.
+  // Folded coset NTT: DFT(x_j s^j) splits at every stage into two half-size problems whose
+  // cosets differ by the stage's twiddle, so each block twiddle of stage u gains the factor
+  // s^(2^(L-1-u)) and the x s^j scaling disappears from the data path.
+  __shared__ uint64_t sig[MAX_TILE_LOG];
+  if (a.fold) {
+    if (threadIdx.x < k) sig[threadIdx.x] = coset_power(a, 1u << (a.log_n - 1 - a.s0 - threadIdx.x));
+    __syncthreads();
+  }
   for (uint32_t idx = threadIdx.x; idx + 1 < (1u << k); idx += blockDim.x) {
     const uint32_t t = 31 - __clz(idx + 1);
     const uint32_t m = idx + 1 - (1u << t);
-    tws[idx] = a.tw[((uint64_t)hi << t) + m];
+    const uint64_t w = a.tw[((uint64_t)hi << t) + m];
+    tws[idx] = a.fold ? mul(w, sig[t]) : w;
   }
   // Coset / size scaling as two per-CTA tables: the exponent j of element (mid, w) splits as
   //   natural j = mid * M + (lo0 + w)                      (strided pass, hi = 0)
@@ -139,7 +150,7 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) ntt_pass_kernel(const PassArg
   // so the factor is P[mid] * Q[w] (P carries N^-1 on the inverse side): 2 multiplies per element.
   uint64_t *Pt = tws + (1u << k);
   uint64_t *Qt = Pt + (1u << k);
-  if (a.scale) {
+  if (a.scale == 1 || (a.scale == 2 && a.log_ext)) {
     for (uint32_t m = threadIdx.x; m < (1u << k); m += blockDim.x) {
       const uint32_t jm = a.j_bitrev ? brev_low(m, k) << (a.log_n - k) : m << log_m;
       const uint64_t pm = coset_power(a, jm);
@@ -180,8 +191,9 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) ntt_pass_kernel(const PassArg
     for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
       const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
       uint64_t v = tile[swz(e)];
-      if (a.scale == 2) v = mul(v, mul(Pt[e >> log_w], Qt[a.j_bitrev ? 0u : (e & wmask)]));
-      dst[i] = canon(v);
+      if (a.scale == 2)
+        v = a.log_ext ? mul(v, mul(Pt[e >> log_w], Qt[a.j_bitrev ? 0u : (e & wmask)])) : mul(v, a.n_inv);
+      dst[i] = a.last ? canon(v) : v;  // a following pass accepts any value below 2^64
     }
   }
 }
@@ -348,7 +360,12 @@ int ntt_launch(const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_n
       a.w_lo = t->w_lo;
       a.w_hi = t->w_hi;
       const bool first = q == 0, last = q + 1 == np;
-      if (!inverse && first && log_ext > 0) {
+      a.last = last ? 1 : 0;
+      if (!inverse && log_ext > 0 && !bitrev_inputs) {
+        a.fold = 1;  // every pass: the coset factor rides on the block twiddles
+        a.g_lo = t->g_lo;
+        a.g_hi = t->g_hi;
+      } else if (!inverse && first && log_ext > 0) {
         a.scale = 1;
         a.j_bitrev = bitrev_inputs ? 1 : 0;  // b2n input position i holds coefficient bitrev(i)
         a.g_lo = t->g_lo;
