@@ -365,6 +365,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": WORKLOAD, "columns": COLS, "log_rows": LOG_N, "lde_factor": f, "cap": 1 << LOG_CAP,
                    "parallelism": "replicas" if world > 1 else "single", "l2": "inputs 1 GiB > 126 MB L2, no flush"},
         "hashes_per_s": (units["perms_leaves"] + units["perms_nodes"]) * world / (ms / 1e3),
+        "algorithmic_gbs": units["bytes"] * world / (ms / 1e3) / 1e9,
         "stages_ms": {k: v / args.steps for k, v in stage.items()},
         "roofline": {"bound": "int", "kernel": "p2_leaves_kernel", "achieved": achieved,
                      "peak": mm_peak / 1e9, "unit": "Gmodmul/s", "frac": achieved * 1e9 / mm_peak,
@@ -599,6 +600,36 @@ def run_serve(args):
     ctx.destroy()
 
 
+def run_ef(args):
+    """Extension-field layout conversion of the 24 extension columns of the 2^22-row trace
+    (vectorized <-> tuples, 16 bytes read + 16 written per element): HBM roofline."""
+    glc, torch, ctx = _setup_device()
+    syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
+    rows, cols = 1 << 22, 24
+    v = torch.empty(2 * cols * rows, dtype=torch.int64, device="cuda")
+    syn.fill_device(v, "ef")
+    t = torch.empty_like(v)
+    peaks, kind = measured_peaks()
+    out = {"workload": "GoldilocksExt2 layouts: 24 extension columns x 2^22 rows", "hbm_gbs_peak": peaks["hbm_gbs"],
+           "peak_source": kind}
+    for name, fn, a, b in (("vectorized_to_tuples", glc.extension_field.vectorized_to_tuples, v, t),
+                           ("tuples_to_vectorized", glc.extension_field.tuples_to_vectorized, t, v)):
+        for _ in range(args.warmup):
+            fn(a, b, rows, cols)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn(a, b, rows, cols)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        gbs = 32 * rows * cols / (ms / 1e3) / 1e9
+        out[name] = {"ms": ms, "GB/s": gbs, "frac_of_hbm": gbs / peaks["hbm_gbs"]}
+    print(json.dumps(out), flush=True)
+    ctx.destroy()
+
+
 def run_profile_case(args):
     """A small commitment for profiler captures: 128 columns x 2^log_n rows (default 2^18, 256 MiB of
     inputs, still larger than L2), LDE x2, cap 16; warm-up plus a few plain glc_commit calls."""
@@ -632,7 +663,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-ref-kernels", action="store_true")
-    ap.add_argument("--workload", default="commit", choices=["commit", "uneven", "large", "serve", "profile"],
+    ap.add_argument("--workload", default="commit", choices=["commit", "uneven", "large", "serve", "profile", "ef"],
                     help="commit: the contract line; others print their own JSON")
     ap.add_argument("--log-n", type=int, default=18, help="rows of the profile case (log2)")
     ap.add_argument("--streams", type=int, default=8)
@@ -643,7 +674,7 @@ def main():
     args = ap.parse_args()
     if args.workload != "commit":
         {"uneven": run_uneven, "large": run_large, "serve": run_serve,
-         "profile": run_profile_case}[args.workload](args)
+         "profile": run_profile_case, "ef": run_ef}[args.workload](args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

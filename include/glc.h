@@ -112,6 +112,16 @@ glc_status glc_poseidon2_gather_merkle_paths(const uint32_t *indexes, size_t ind
                                              size_t values_len, uint64_t *results, size_t results_len,
                                              uint32_t layers_count, void *stream);
 
+/* GoldilocksExt2 column layouts, replacing extension_field::convert (extension_field.rs:60-90,
+ * kernels goldilocks_extension.cu:8-34).  Vectorized: extension column k is two base columns, c0 at
+ * v[2k*v_stride + row] and c1 at v[(2k+1)*v_stride + row] (strides in base elements).  Tuples:
+ * element (row, k) is the pair {c0, c1} at t[2*(k*t_stride + row)] (strides in extension
+ * elements; the tuple matrix must be 16-byte aligned).  Strides >= rows. */
+glc_status glc_ef_vectorized_to_tuples(const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint64_t dst_stride,
+                                       uint32_t rows, uint32_t cols, void *stream);
+glc_status glc_ef_tuples_to_vectorized(const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint64_t dst_stride,
+                                       uint32_t rows, uint32_t cols, void *stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Commitment jobs (no single counterpart in boojum-cuda: this is the sequence shivini runs for one
  * trace / argument / quotient commitment, crates/shivini/src/data_structures/storage.rs:155-330,

@@ -255,6 +255,26 @@ void or_bit_reverse(const uint64_t *src, uint64_t src_stride, uint64_t *dst, uin
   free(tmp);
 }
 
+/* GoldilocksExt2 layout conversions (goldilocks_extension.cu:8-34: element (row, col) read
+ * through one accessor and written through the other). */
+void or_ef_vectorized_to_tuples(const uint64_t *v, uint64_t v_stride, uint64_t *t, uint64_t t_stride, uint32_t rows,
+                                uint32_t cols) {
+  for (uint64_t k = 0; k < cols; k++)
+    for (uint64_t r = 0; r < rows; r++) {
+      t[2 * (k * t_stride + r)] = v[2 * k * v_stride + r];
+      t[2 * (k * t_stride + r) + 1] = v[(2 * k + 1) * v_stride + r];
+    }
+}
+
+void or_ef_tuples_to_vectorized(const uint64_t *t, uint64_t t_stride, uint64_t *v, uint64_t v_stride, uint32_t rows,
+                                uint32_t cols) {
+  for (uint64_t k = 0; k < cols; k++)
+    for (uint64_t r = 0; r < rows; r++) {
+      v[2 * k * v_stride + r] = t[2 * (k * t_stride + r)];
+      v[(2 * k + 1) * v_stride + r] = t[2 * (k * t_stride + r) + 1];
+    }
+}
+
 /* ------------------------------------------------------------------------------------------
  * Poseidon2 over Goldilocks, width 12, rate 8, capacity 4, x^7, 4+4 full and 22 partial
  * rounds (crates/boojum-cuda/native/poseidon2/gl/poseidon2_gl_st.cu:9-23,

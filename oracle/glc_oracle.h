@@ -93,6 +93,15 @@ int64_t or_p2_find_opening(const uint64_t *leaf, uint32_t leaf_len, const uint64
  *          lde_out + c*cols*2^log_n and uses kernel coset index bitrev(c).
  * trees_out: one Merkle subtree per coset, each 2*4*2^log_n entries, subtree cap 2^(log_cap-log_lde).
  * cap_out: 4*2^log_cap entries, [4][cap] layout (coset caps concatenated). */
+/* GoldilocksExt2 column layouts (crates/boojum-cuda/src/extension_field.rs:60-90,
+ * native/goldilocks_extension.cu:8-34, native/memory.cuh:545-612).  Vectorized: extension column
+ * k is two base columns, c0 at v[2*k*v_stride + row] and c1 at v[(2*k+1)*v_stride + row].
+ * Tuples: element (row, k) is the pair {c0, c1} at t[2*(k*t_stride + row)]. */
+void or_ef_vectorized_to_tuples(const uint64_t *v, uint64_t v_stride, uint64_t *t, uint64_t t_stride, uint32_t rows,
+                                uint32_t cols);
+void or_ef_tuples_to_vectorized(const uint64_t *t, uint64_t t_stride, uint64_t *v, uint64_t v_stride, uint32_t rows,
+                                uint32_t cols);
+
 int or_commit(const uint64_t *evals, uint32_t log_n, uint32_t cols, uint32_t log_lde, uint32_t log_cap,
               uint64_t *monomials_out, uint64_t *lde_out, uint64_t *trees_out, uint64_t *cap_out, int threads);
 

@@ -41,6 +41,8 @@ def lib():
         L.or_batch_ntt.argtypes = ntt_args + [C.c_int]
         L.or_batch_ntt_naive.argtypes = ntt_args
         L.or_bit_reverse.argtypes = [u64p, C.c_uint64, u64p, C.c_uint64, C.c_uint32, C.c_uint32]
+        L.or_ef_vectorized_to_tuples.argtypes = [u64p, C.c_uint64, u64p, C.c_uint64, C.c_uint32, C.c_uint32]
+        L.or_ef_tuples_to_vectorized.argtypes = [u64p, C.c_uint64, u64p, C.c_uint64, C.c_uint32, C.c_uint32]
         L.or_p2_set_round_constants.argtypes = [u64p]
         L.or_p2_permutation.argtypes = [u64p]
         L.or_p2_leaves.argtypes = [u64p, sz, u64p, sz, C.c_uint32, C.c_int, C.c_int, C.c_int]
@@ -108,6 +110,21 @@ def bit_reverse(src, log_rows, cols, src_stride=None, dst=None, dst_stride=None)
         dst = np.zeros(cols * dst_stride, dtype=np.uint64)
     lib().or_bit_reverse(_p(src), src_stride, _p(dst), dst_stride, log_rows, cols)
     return dst
+
+
+def ef_vectorized_to_tuples(v, v_stride, rows, cols, t_stride=None):
+    """GoldilocksExt2 columns: vectorized (c0 column, c1 column) -> {c0, c1} pairs."""
+    t_stride = rows if t_stride is None else t_stride
+    t = np.zeros(2 * cols * t_stride, dtype=np.uint64)
+    lib().or_ef_vectorized_to_tuples(_p(v), v_stride, _p(t), t_stride, rows, cols)
+    return t
+
+
+def ef_tuples_to_vectorized(t, t_stride, rows, cols, v_stride=None):
+    v_stride = rows if v_stride is None else v_stride
+    v = np.zeros(2 * cols * v_stride, dtype=np.uint64)
+    lib().or_ef_tuples_to_vectorized(_p(t), t_stride, _p(v), v_stride, rows, cols)
+    return v
 
 
 def leaves(values, results_len, log_rows_per_hash=0, load_intermediate=False, store_intermediate=False,

@@ -246,3 +246,17 @@ def test_commit_matches_steps(oracle):
     big = oracle.build_merkle_tree(np.ascontiguousarray(all_leaves.reshape(-1)), 8 * 2 * n, 0, log_n + 1 - log_cap + 2)
     cap_off = 8 * 2 * n - 8 * (1 << log_cap)
     assert (big[cap_off:cap_off + 4 * (1 << log_cap)] == cap).all()
+
+
+def test_extension_layouts(oracle):
+    # vectorized column k = base columns 2k (c0) and 2k+1 (c1), stride 7; tuples stride 5
+    # (memory.cuh:545-612 accessors: c1 sits one stride after c0, a column step is two strides)
+    v = np.arange(2 * 3 * 7, dtype=np.uint64)
+    t = oracle.ef_vectorized_to_tuples(v, 7, 5, 3, 5)
+    want = []
+    for k in range(3):
+        for r in range(5):
+            want += [2 * k * 7 + r, (2 * k + 1) * 7 + r]
+    assert t.tolist() == want
+    back = oracle.ef_tuples_to_vectorized(t, 5, 5, 3, 7).reshape(6, 7)
+    assert (back[:, :5] == v.reshape(6, 7)[:, :5]).all() and (back[:, 5:] == 0).all()

@@ -1,7 +1,8 @@
 """ctypes binding of libglc.so (the C ABI declared in include/glc.h).
 
 The library must have been built (build.py); loading fails loudly otherwise: there is no CPU
-fallback for any entry point.
+fallback for any entry point.  GLC_LIBRARY names another build of the same library to load
+instead of _build/libglc.so.
 """
 from __future__ import annotations
 
@@ -9,7 +10,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_build", "libglc.so")
+LIB_PATH = os.environ.get("GLC_LIBRARY") or os.path.join(HERE, "_build", "libglc.so")
 
 
 class GlcError(RuntimeError):
@@ -47,6 +48,8 @@ SIGNATURES = {
     "glc_poseidon2_build_merkle_tree": (C.c_int, [u64p, sz, u64p, sz, u32, u32, vp]),
     "glc_poseidon2_gather_rows": (C.c_int, [u32p, sz, u32, u64p, u64, u64, u64, u64p, u64, u64, u64, vp]),
     "glc_poseidon2_gather_merkle_paths": (C.c_int, [u32p, sz, u64p, sz, u64p, sz, u32, vp]),
+    "glc_ef_vectorized_to_tuples": (C.c_int, [u64p, u64, u64p, u64, u32, u32, vp]),
+    "glc_ef_tuples_to_vectorized": (C.c_int, [u64p, u64, u64p, u64, u32, u32, vp]),
     "glc_commit": (C.c_int, [vp, vp]),
     "glc_commit_profiled": (C.c_int, [vp, vp, vp, u32]),
     "glc_commit_cap_noalloc": (C.c_int, [u64p, u64, u32, u32, u32, u32, u64p, vp]),
