@@ -341,6 +341,17 @@ def run_ours(args, rank, world, local_rank):
     leaf_ms = stage["leaves"] / (args.steps * f)  # per launch
     leaf_modmul = MODMUL_PER_PERM * units["perms_leaves"] / f
     achieved = leaf_modmul / (leaf_ms / 1e3) / 1e9
+    # the same leaf launch alone on the stream (in the step it shares the GPU with the other
+    # coset's NTT, which stretches its duration): one coset of the LDE, 3 launches, events
+    lr = []
+    for _ in range(3):
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        glc.GLHasher.compute_leaf_hashes(job.lde[:COLS << LOG_N], job.trees[:4 << LOG_N], 0, False, False)
+        a1.record()
+        torch.cuda.synchronize()
+        lr.append(a0.elapsed_time(a1))
+    leaf_alone_ms = statistics.median(lr)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
@@ -369,6 +380,8 @@ def run_ours(args, rank, world, local_rank):
         "stages_ms": {k: v / args.steps for k, v in stage.items()},
         "roofline": {"bound": "int", "kernel": "p2_leaves_kernel", "achieved": achieved,
                      "peak": mm_peak / 1e9, "unit": "Gmodmul/s", "frac": achieved * 1e9 / mm_peak,
+                     "launch_ms_in_step": leaf_ms, "launch_ms_alone": leaf_alone_ms,
+                     "frac_alone": leaf_modmul / (leaf_alone_ms / 1e3) / mm_peak,
                      "traffic": traffic,
                      "peak_source": "glc_modmul_probe measured live in this run (8 independent chains per thread)"},
         "roofline_job": {"bytes": units["bytes"], "modmul": units["modmul"], "t_roof_ms": t_roof * 1e3,
