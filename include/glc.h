@@ -229,7 +229,7 @@ typedef struct glc_ntt_tuning {
   uint32_t k1;               /* stages in the strided pass of a two-pass NTT (0 = log_n / 2) */
   uint32_t max_log_w;        /* tile rows hold up to 2^max_log_w contiguous elements (<= 5) */
   uint32_t max_cols_per_cta; /* columns one CTA walks with the same twiddles (1..64) */
-  uint32_t l2_chunk_mb;      /* a two-pass NTT runs both passes per chunk of this many MiB */
+  uint32_t l2_chunk_mb;      /* a two-pass NTT runs both passes per chunk of this many MiB; 0: one chunk */
 } glc_ntt_tuning;
 typedef struct glc_p2_tuning {
   uint32_t leaf_threads; /* 64, 128 or 256 (leaf and wide node-layer kernels) */
@@ -241,8 +241,9 @@ glc_status glc_tuning_get_ntt(uint32_t log_n, glc_ntt_tuning *out);
 glc_status glc_tuning_set_ntt(uint32_t log_n, const glc_ntt_tuning *tuning);
 glc_status glc_tuning_get_p2(glc_p2_tuning *out);
 glc_status glc_tuning_set_p2(const glc_p2_tuning *tuning);
-/* Times the candidates for log_n in [log_n_min, log_n_max] on `cols` columns (synchronous;
- * allocates and frees a scratch buffer of cols << log_n_max elements). */
+/* Times the candidates for log_n in [log_n_min, log_n_max] on `cols` columns, or with cols = 0 on
+ * 128 columns capped at 2^28 elements per size (synchronous; allocates and frees one scratch
+ * buffer of the largest batch, at least 132 x 2^19 elements). */
 glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint32_t cols, uint32_t reps);
 glc_status glc_tuning_save(const char *path);
 glc_status glc_tuning_load(const char *path);

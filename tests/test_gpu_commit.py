@@ -92,14 +92,15 @@ def test_commit_contract(glc, syn):
         glc.commit.commit(job)
 
 
-@pytest.mark.parametrize("radix,k1,lw,cpc", [(2, 0, 5, 8), (3, 7, 3, 1), (4, 12, 4, 4), (3, 10, 5, 64)])
-def test_ntt_tuning_invariance(glc, oracle, radix, k1, lw, cpc):
+@pytest.mark.parametrize("radix,k1,lw,cpc,mb", [(2, 0, 5, 8, 8), (3, 7, 3, 1, 8), (4, 12, 4, 4, 0), (3, 10, 5, 64, 0),
+                                                (4, 9, 3, 8, 0)])
+def test_ntt_tuning_invariance(glc, oracle, radix, k1, lw, cpc, mb):
     """Every tuning choice computes the same transform (bit-exact)."""
     log_n = 20 if k1 != 7 else 14
     n = 1 << log_n
     cols = 3
     saved = glc.tuning.get_ntt(log_n)
-    glc.tuning.set_ntt(log_n, radix, k1, lw, cpc, 8)
+    glc.tuning.set_ntt(log_n, radix, k1, lw, cpc, mb)
     try:
         x = syn_x = load_synthetic().random_field_elements("tune-%d" % radix, cols * n)
         for bitrev_inputs, inverse, e, c in ((False, False, 1, 1), (True, True, 2, 3)):

@@ -41,7 +41,7 @@ extern "C" glc_status glc_tuning_get_ntt(uint32_t log_n, glc_ntt_tuning *out) {
 extern "C" glc_status glc_tuning_set_ntt(uint32_t log_n, const glc_ntt_tuning *in) {
   if (!in || log_n < 1 || log_n > MAX_LOG_N) return fail("tuning: bad arguments");
   if (in->radix_bits < 2 || in->radix_bits > 4) return fail("tuning: radix_bits must be 2, 3 or 4");
-  if (in->max_log_w > 5 || in->max_cols_per_cta == 0 || in->max_cols_per_cta > 64 || in->l2_chunk_mb == 0)
+  if (in->max_log_w > 5 || in->max_cols_per_cta == 0 || in->max_cols_per_cta > 64)
     return fail("tuning: values out of range");
   if (in->k1 && (in->k1 > 12 || log_n - in->k1 > 12 || in->k1 >= log_n)) return fail("tuning: k1 out of range");
   NttTuning &t = ntt_tuning(log_n);
@@ -74,14 +74,19 @@ extern "C" glc_status glc_tuning_set_p2(const glc_p2_tuning *in) {
 }
 
 extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint32_t cols, uint32_t reps) {
-  if (log_n_min < 1 || log_n_max > MAX_LOG_N || log_n_min > log_n_max || cols == 0)
+  if (log_n_min < 1 || log_n_max > MAX_LOG_N || log_n_min > log_n_max || cols > 65536)
     return fail("autotune: bad size range");
   if (!current_tables()) return fail("autotune: glc_context_create has not been called on this device");
   if (reps == 0) reps = 3;
+  // cols == 0: a commitment-sized batch per size, 128 columns up to 2^28 elements (2 GiB)
+  auto cols_for = [&](uint32_t log_n) -> uint32_t {
+    return cols ? cols : (uint32_t)std::min<uint64_t>(128, std::max<uint64_t>(8, (1ull << 28) >> log_n));
+  };
   // scratch: the largest NTT batch, and the leaf probe's 128 x 2^19 values (larger than L2, many
   // column streams, like a real commitment) + 4 x 2^17 digests
   constexpr uint64_t LEAF_ROWS = 1ull << 19, LEAF_COLS = 128;
-  const uint64_t elems = std::max<uint64_t>((uint64_t)cols << log_n_max, (LEAF_COLS + 4) * LEAF_ROWS);
+  uint64_t elems = (LEAF_COLS + 4) * LEAF_ROWS;
+  for (uint32_t l = log_n_min; l <= log_n_max; l++) elems = std::max<uint64_t>(elems, (uint64_t)cols_for(l) << l);
   uint64_t *buf = nullptr;
   cudaError_t ce = cudaMalloc(&buf, elems * sizeof(uint64_t));
   if (ce != cudaSuccess) return (int)ce;
@@ -98,22 +103,28 @@ extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint3
     const NttTuning saved = ntt_tuning(log_n);
     NttTuning best = saved;
     float best_ms = 1e30f;
+    const uint32_t nc = cols_for(log_n);
+    // strided-pass stages within 3 of an even split (0 = the default split)
     std::vector<uint32_t> k1s = {0};
     if (log_n > 12)
-      for (uint32_t k = std::max(log_n - 12, 1u); k <= std::min(12u, log_n - 1); k++) k1s.push_back(k);
+      for (uint32_t k = std::max(log_n - 12, 1u); k <= std::min(12u, log_n - 1); k++)
+        if (k + 3 >= log_n / 2 && k <= log_n / 2 + 3) k1s.push_back(k);
     for (uint32_t rb : {2u, 3u, 4u})
       for (uint32_t k1 : k1s)
         for (uint32_t lw : {3u, 4u, 5u})
-          for (uint32_t cpc : {1u, 4u, 8u}) {
+          for (uint32_t cpc : {1u, 4u, 8u})
+            for (uint32_t mb : {0u, 48u}) {
+            if (err || (mb && log_n <= 12)) continue;  // stop after an error; one pass: nothing to chunk
             NttTuning c = saved;
             c.radix_bits = rb;
             c.k1 = k1;
             c.max_log_w = lw;
             c.max_cols_per_cta = cpc;
+            c.l2_chunk_mb = mb;
             ntt_tuning(log_n) = c;
             // time a forward coset LDE (the commitment's dominant NTT), in place
             const float ms = time_ms(s, (int)reps, [&] {
-              return ntt_launch(buf, buf, log_n, cols, 1ull << log_n, 1ull << log_n, false, false, 1, 1, s, 0);
+              return ntt_launch(buf, buf, log_n, nc, 1ull << log_n, 1ull << log_n, false, false, 1, 1, s, 0);
             }, &err);
             if (err) break;
             if (ms < best_ms) {
@@ -133,6 +144,7 @@ extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint3
       for (uint32_t rolled : {0u, 1u, 2u})
         for (bool lazy : {false, true})
           for (uint32_t minb : {2u, 3u}) {
+        if (err) continue;
         P2Tuning c;
         c.leaf_threads = th;
         c.rolled = rolled;

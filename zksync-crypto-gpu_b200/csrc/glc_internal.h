@@ -54,7 +54,7 @@ struct NttTuning {
   uint32_t k1 = 0;                // stages in the strided pass of a two-pass plan (0: log_n / 2)
   uint32_t max_log_w = 5;         // at most 2^max_log_w contiguous elements per tile row
   uint32_t max_cols_per_cta = 8;  // columns one CTA walks with the same twiddles
-  uint32_t l2_chunk_mb = 48;      // columns per L2-resident chunk of a two-pass NTT
+  uint32_t l2_chunk_mb = 0;       // columns per L2-resident chunk of a two-pass NTT (0: all columns)
 };
 NttTuning &ntt_tuning(uint32_t log_n);
 

@@ -334,8 +334,10 @@ int ntt_launch(const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_n
   const uint64_t n = 1ull << log_n;
   if (l2_chunk_cols == 0) {
     // keep one chunk of columns resident in L2 across the passes
+    // (chunking trades HBM traffic for CTAs that each cover fewer columns and rebuild their
+    // twiddles more often; on B200 the NTT is integer-bound, so one chunk usually wins)
     const uint64_t budget = (uint64_t)tu.l2_chunk_mb << 20;
-    l2_chunk_cols = (uint32_t)std::max<uint64_t>(1, budget / (n * 8));
+    l2_chunk_cols = tu.l2_chunk_mb ? (uint32_t)std::max<uint64_t>(1, budget / (n * 8)) : num_ntts;
   }
   if (np == 1) l2_chunk_cols = num_ntts;
   for (uint32_t c0 = 0; c0 < num_ntts; c0 += l2_chunk_cols) {

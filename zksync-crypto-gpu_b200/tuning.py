@@ -21,7 +21,7 @@ def get_ntt(log_n: int) -> NttTuning:
     return t
 
 
-def set_ntt(log_n: int, radix_bits=3, k1=0, max_log_w=5, max_cols_per_cta=8, l2_chunk_mb=48) -> None:
+def set_ntt(log_n: int, radix_bits=3, k1=0, max_log_w=5, max_cols_per_cta=8, l2_chunk_mb=0) -> None:
     t = NttTuning(radix_bits, k1, max_log_w, max_cols_per_cta, l2_chunk_mb)
     call("glc_tuning_set_ntt", log_n, C.byref(t))
 
@@ -37,7 +37,9 @@ def set_p2(leaf_threads=256, rolled=1, lazy=0, min_blocks=2) -> None:
     call("glc_tuning_set_p2", C.byref(t))
 
 
-def autotune(log_n_min: int, log_n_max: int, cols: int = 16, reps: int = 3) -> None:
+def autotune(log_n_min: int, log_n_max: int, cols: int = 0, reps: int = 3) -> None:
+    """Time the launch candidates on this device and install the fastest (cols = 0: 128 columns,
+    capped at 2^28 elements per size)."""
     call("glc_autotune", log_n_min, log_n_max, cols, reps)
 
 
