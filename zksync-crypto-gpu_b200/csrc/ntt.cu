@@ -15,8 +15,10 @@
 //    use the twiddle T[b] = w^bitrev(b) of block b at each stage; T is one flat table.
 //  * Coset scaling (forward LDE: x s^j on load) and N^-1 s^-j (inverse: on store) are fused
 //    into the first / last pass, so an LDE costs no extra HBM pass.
-//  * Batches larger than an L2-sized chunk of columns run pass 1 and pass 2 chunk by chunk, so
-//    the second pass reads the first pass's output from the 126 MB L2 instead of HBM.
+//  * Optionally (tuning), batches larger than an L2-sized chunk of columns run pass 1 and pass 2
+//    chunk by chunk, so the second pass reads the first pass's output from the 126 MB L2.  The
+//    NTT is integer-bound, and small chunks cost more in per-CTA twiddle tables than they save
+//    in HBM traffic, so the default is one chunk.
 #include <algorithm>
 
 #include "glc_field.cuh"
