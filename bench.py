@@ -618,12 +618,13 @@ def run_ef(args):
     (vectorized <-> tuples, 16 bytes read + 16 written per element): HBM roofline."""
     glc, torch, ctx = _setup_device()
     syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
-    rows, cols = 1 << 22, 24
+    rows, cols = 1 << args.ef_log_rows, 24
     v = torch.empty(2 * cols * rows, dtype=torch.int64, device="cuda")
     syn.fill_device(v, "ef")
     t = torch.empty_like(v)
     peaks, kind = measured_peaks()
-    out = {"workload": "GoldilocksExt2 layouts: 24 extension columns x 2^22 rows", "hbm_gbs_peak": peaks["hbm_gbs"],
+    out = {"workload": "GoldilocksExt2 layouts: 24 extension columns x 2^%d rows" % args.ef_log_rows,
+           "hbm_gbs_peak": peaks["hbm_gbs"],
            "peak_source": kind}
     for name, fn, a, b in (("vectorized_to_tuples", glc.extension_field.vectorized_to_tuples, v, t),
                            ("tuples_to_vectorized", glc.extension_field.tuples_to_vectorized, t, v)):
@@ -679,6 +680,7 @@ def main():
     ap.add_argument("--workload", default="commit", choices=["commit", "uneven", "large", "serve", "profile", "ef"],
                     help="commit: the contract line; others print their own JSON")
     ap.add_argument("--log-n", type=int, default=18, help="rows of the profile case (log2)")
+    ap.add_argument("--ef-log-rows", type=int, default=22, help="rows of the extension-layout workload (log2)")
     ap.add_argument("--streams", type=int, default=8)
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--serve-jobs", type=int, default=40)

@@ -42,6 +42,8 @@ struct PassArgs {
   uint32_t scale;     // 0: none, 1: x s^j on load, 2: x N^-1 s^-j on store
   uint32_t fold;      // 1: forward n2b coset NTT with s folded into the block twiddles
   uint32_t last;      // last pass: canonical output
+  uint32_t vec2;      // 16-byte loads and stores: aligned matrices, even strides, no per-element
+                      // coset factor on load, no coset factor on store
   uint32_t j_bitrev;  // exponent j = bitrev_L(position) instead of position
   uint32_t log_ext, coset;
   uint64_t n_inv;
@@ -170,11 +172,22 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) ntt_pass_kernel(const PassArg
     const uint64_t *src = a.in + (uint64_t)col * a.in_stride;
     uint64_t *dst = a.out + (uint64_t)col * a.out_stride;
     __syncthreads();
-    for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
-      const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
-      uint64_t v = src[i];
-      if (a.scale == 1) v = mul(v, mul(Pt[e >> log_w], Qt[a.j_bitrev ? 0u : (e & wmask)]));
-      tile[swz(e)] = v;
+    if (a.vec2) {
+      // two consecutive elements per thread, one 16-byte load: tile indexes e and e + 1 are
+      // adjacent in memory (same row of a W >= 2 tile, or a contiguous W = 1 tile)
+      for (uint32_t e = 2 * threadIdx.x; e < E; e += 2 * blockDim.x) {
+        const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
+        const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(src + i);
+        tile[swz(e)] = v.x;
+        tile[swz(e + 1)] = v.y;
+      }
+    } else {
+      for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
+        const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
+        uint64_t v = src[i];
+        if (a.scale == 1) v = mul(v, mul(Pt[e >> log_w], Qt[a.j_bitrev ? 0u : (e & wmask)]));
+        tile[swz(e)] = v;
+      }
     }
     __syncthreads();
     if (!a.dif) {
@@ -190,12 +203,28 @@ __global__ void __launch_bounds__(PASS_THREADS, 2) ntt_pass_kernel(const PassArg
         __syncthreads();
       }
     }
-    for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
-      const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
-      uint64_t v = tile[swz(e)];
-      if (a.scale == 2)
-        v = a.log_ext ? mul(v, mul(Pt[e >> log_w], Qt[a.j_bitrev ? 0u : (e & wmask)])) : mul(v, a.n_inv);
-      dst[i] = a.last ? canon(v) : v;  // a following pass accepts any value below 2^64
+    if (a.vec2) {
+      for (uint32_t e = 2 * threadIdx.x; e < E; e += 2 * blockDim.x) {
+        const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
+        uint64_t v0 = tile[swz(e)], v1 = tile[swz(e + 1)];
+        if (a.scale == 2) {
+          v0 = mul(v0, a.n_inv);
+          v1 = mul(v1, a.n_inv);
+        }
+        if (a.last) {
+          v0 = canon(v0);
+          v1 = canon(v1);
+        }
+        *reinterpret_cast<ulonglong2 *>(dst + i) = make_ulonglong2(v0, v1);
+      }
+    } else {
+      for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
+        const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
+        uint64_t v = tile[swz(e)];
+        if (a.scale == 2)
+          v = a.log_ext ? mul(v, mul(Pt[e >> log_w], Qt[a.j_bitrev ? 0u : (e & wmask)])) : mul(v, a.n_inv);
+        dst[i] = a.last ? canon(v) : v;  // a following pass accepts any value below 2^64
+      }
     }
   }
 }
@@ -380,6 +409,12 @@ int ntt_launch(const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_n
         a.g_lo = t->gi_lo;
         a.g_hi = t->gi_hi;
       }
+      const bool aligned = ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out)) & 15) == 0 &&
+                           (a.in_stride & 1) == 0 && (a.out_stride & 1) == 0;
+      // pairs of tile indexes (e, e + 1) must be adjacent in memory: rows of W >= 2 elements, or
+      // W = 1 with a contiguous tile (M = 1)
+      const bool pairs_adjacent = ps.log_w >= 1 || log_n - ps.s0 - ps.k == 0;
+      a.vec2 = (aligned && pairs_adjacent && a.scale != 1 && !(a.scale == 2 && log_ext)) ? 1 : 0;
       const uint32_t tile_log = ps.k + ps.log_w;
       const uint64_t tiles_per_col = n >> tile_log;
       // enough CTAs to fill 148 SMs a few times over; the rest of the columns loop inside a CTA
