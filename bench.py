@@ -600,9 +600,11 @@ def run_serve(args):
     make = lambda i, l, c: base[:c << l]
     out = {"workload": "serving: Poisson(%g/s) arrivals, %d jobs, log2 rows U[16,23], columns U[8,256], LDE x2/x4"
                        % (args.rate, len(jobs)), "budget_gb": args.budget_gb}
-    for name, inflight, streams in (("continuous_batching", args.inflight, args.streams), ("plain_sequential", 1, 1)):
+    for name, inflight, streams, prio in (("continuous_batching", args.inflight, args.streams, True),
+                                          ("continuous_batching_flat_priority", args.inflight, args.streams, False),
+                                          ("plain_sequential", 1, 1, False)):
         with glc.serve.Server(hbm_budget_bytes=int(args.budget_gb * (1 << 30)), max_inflight=inflight,
-                              streams=streams) as srv:
+                              streams=streams, size_priority=prio) as srv:
             r = glc.serve.poisson_load(srv, jobs, rate_per_s=args.rate, seed=3, make_input=make)
             st = srv.stats()
         r.pop("caps")

@@ -188,6 +188,8 @@ typedef struct glc_server_config {
   uint64_t hbm_budget_bytes; /* admission limit on the device memory held by admitted requests */
   uint32_t max_inflight;     /* at most this many requests on the device at once */
   uint32_t streams;          /* streams the requests run on (0 = 8) */
+  uint32_t flat_priority;    /* 0: smaller requests run on higher-priority streams (their blocks are
+                                scheduled first as SMs free up); 1: all streams at one priority */
 } glc_server_config;
 typedef struct glc_serve_request {
   const uint64_t *host_evals; /* cols x 2^log_n natural-order evaluations (host) */

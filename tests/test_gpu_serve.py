@@ -22,11 +22,13 @@ def inp(i, log_n, cols):
     return load_synthetic().random_field_elements("serve-%d" % i, cols << log_n)
 
 
-def test_mix_equals_alone(glc, oracle):
-    # the first job runs long enough that the small ones arrive while it is on the device
+@pytest.mark.parametrize("size_priority", [True, False])
+def test_mix_equals_alone(glc, oracle, size_priority):
+    # the first job runs long enough that the small ones arrive while it is on the device; with
+    # size priorities the small ones run on higher-priority streams than the first
     jobs = [(18, 64, 1, 4), (12, 8, 1, 4), (14, 24, 2, 4), (13, 16, 1, 4), (12, 40, 2, 4), (15, 8, 1, 4),
             (12, 130, 1, 1)]
-    with glc.serve.Server(hbm_budget_bytes=8 << 30, max_inflight=4, streams=4) as srv:
+    with glc.serve.Server(hbm_budget_bytes=8 << 30, max_inflight=4, streams=4, size_priority=size_priority) as srv:
         res = glc.serve.poisson_load(srv, jobs, rate_per_s=0, make_input=inp)
         st = srv.stats()
     assert st["completed"] >= len(jobs) and st["peak_inflight"] > 1, st

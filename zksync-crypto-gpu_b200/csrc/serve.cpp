@@ -43,6 +43,8 @@ struct Server {
   int device = 0;
   std::vector<cudaStream_t> streams;
   std::vector<uint32_t> stream_load;
+  std::vector<uint32_t> stream_class;  // 0 = highest priority
+  uint32_t classes = 1;
   cudaStream_t copy_stream = nullptr;  // result copies to the host
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -76,13 +78,28 @@ static int request_check(const glc_serve_request &r) {
   return commit_check(j);
 }
 
+// Priority class of a request: its footprint against the budget, in factors of 4 (below 1/64,
+// 1/16, 1/4, above), so a small job's kernels are not queued behind a large job's blocks.
+static uint32_t request_class(const Server &s, uint64_t footprint) {
+  uint32_t c = 0;
+  for (uint64_t edge = s.cfg.hbm_budget_bytes / 64; c + 1 < s.classes && footprint >= edge; edge *= 4) c++;
+  return c;
+}
+
 // Allocates and enqueues one admitted request (worker thread, lock held by the caller).
 static int start_request(Server &s, Request &q) {
   const glc_serve_request &r = q.req;
   const uint64_t n = 1ull << r.log_n, f = 1ull << r.log_lde;
-  int best = 0;
-  for (size_t i = 1; i < s.streams.size(); i++)
-    if (s.stream_load[i] < s.stream_load[best]) best = (int)i;
+  // least-loaded stream of the request's priority class (any stream when none has that class)
+  const uint32_t cls = request_class(s, q.footprint);
+  int best = -1;
+  for (size_t i = 0; i < s.streams.size(); i++)
+    if (s.stream_class[i] == cls && (best < 0 || s.stream_load[i] < s.stream_load[best])) best = (int)i;
+  if (best < 0) {
+    best = 0;
+    for (size_t i = 1; i < s.streams.size(); i++)
+      if (s.stream_load[i] < s.stream_load[best]) best = (int)i;
+  }
   q.stream = best;
   cudaStream_t st = s.streams[best];
   cudaError_t e = cudaSuccess;
@@ -216,9 +233,16 @@ extern "C" glc_status glc_server_create(const glc_server_config *config, glc_ser
     delete srv;
     return fail("serve: cannot create the copy stream");
   }
+  // stream priorities: up to 4 classes from the device's range (greatest is numerically lowest)
+  int least = 0, greatest = 0;
+  if (!s.cfg.flat_priority && cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess)
+    s.classes = std::max<uint32_t>(1, std::min<uint32_t>({4u, (uint32_t)(least - greatest + 1), s.cfg.streams}));
   for (uint32_t i = 0; i < s.cfg.streams; i++) {
     cudaStream_t st;
-    const cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    const uint32_t cls = i % s.classes;
+    const int prio = s.classes > 1 ? greatest + (int)(cls * (uint32_t)(least - greatest) / (s.classes - 1)) : 0;
+    const cudaError_t e = s.classes > 1 ? cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio)
+                                        : cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
       for (auto x : s.streams) cudaStreamDestroy(x);
       delete srv;
@@ -226,6 +250,7 @@ extern "C" glc_status glc_server_create(const glc_server_config *config, glc_ser
     }
     s.streams.push_back(st);
     s.stream_load.push_back(0);
+    s.stream_class.push_back(cls);
   }
   s.worker = std::thread(worker_main, &s);
   *out = srv;

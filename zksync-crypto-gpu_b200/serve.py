@@ -12,7 +12,8 @@ from ._lib import GlcError, call, lib
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_inflight", C.c_uint32), ("streams", C.c_uint32)]
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_inflight", C.c_uint32), ("streams", C.c_uint32),
+                ("flat_priority", C.c_uint32)]
 
 
 class ServeRequest(C.Structure):
@@ -61,10 +62,10 @@ class Pending:
 class Server:
     """Owns a glc_server on the current device.  submit() takes host numpy arrays (uint64)."""
 
-    def __init__(self, hbm_budget_bytes: int, max_inflight: int = 16, streams: int = 8):
+    def __init__(self, hbm_budget_bytes: int, max_inflight: int = 16, streams: int = 8, size_priority: bool = True):
         _bind()
         self._h = C.c_void_p()
-        cfg = ServerConfig(hbm_budget_bytes, max_inflight, streams)
+        cfg = ServerConfig(hbm_budget_bytes, max_inflight, streams, 0 if size_priority else 1)
         call("glc_server_create", C.byref(cfg), C.byref(self._h))
         self._pending: dict[int, Pending] = {}
 
