@@ -67,7 +67,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
         except Exception:
@@ -77,7 +77,15 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
-    def stop(self):
+    def wait_first(self, timeout_s=3.0):
+        """Block until the sampler has produced a line (nvidia-smi takes a moment to start), so
+        the timed region is covered; returns the index of the next sample."""
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < timeout_s:
+            time.sleep(0.01)
+        return len(self.lines)
+
+    def stop(self, since=0):
         if self.proc:
             self.proc.terminate()
             try:
@@ -86,7 +94,7 @@ class ClockSampler:
                 self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
+        for l in self.lines[since:]:
             parts = [p.strip() for p in l.split(",")]
             if len(parts) < 8:
                 continue
@@ -236,6 +244,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- timed region: inputs resident in HBM ----
     clocks = ClockSampler(local_rank)
     clocks.start()
+    i_clk = clocks.wait_first()
     stage = {"monomials": 0.0, "ntt": 0.0, "leaves": 0.0, "nodes": 0.0, "caps": 0.0}
     l0 = lib.glc_launch_count()
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -254,7 +263,7 @@ def run_ours(args, rank, world, local_rank):
     t_end.record()
     torch.cuda.synchronize()
     launches = (lib.glc_launch_count() - l0) // max(1, args.steps)
-    clk = clocks.stop()
+    clk = clocks.stop(since=i_clk)
     barrier()
     ms = t_start.elapsed_time(t_end) / args.steps
     if world > 1:
@@ -381,6 +390,8 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "int", "kernel": "p2_leaves_kernel", "achieved": achieved,
                      "peak": mm_peak / 1e9, "unit": "Gmodmul/s", "frac": achieved * 1e9 / mm_peak,
                      "launch_ms_in_step": leaf_ms, "launch_ms_alone": leaf_alone_ms,
+                     "hbm_gbs_alone": (traffic or 0) / (leaf_alone_ms / 1e3) / 1e9,
+                     "hbm_frac_alone": (traffic or 0) / (leaf_alone_ms / 1e3) / 1e9 / peaks["hbm_gbs"],
                      "frac_alone": leaf_modmul / (leaf_alone_ms / 1e3) / mm_peak,
                      "traffic": traffic,
                      "peak_source": "glc_modmul_probe measured live in this run (8 independent chains per thread)"},
@@ -675,7 +686,7 @@ def run_profile_case(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-ref-kernels", action="store_true")

@@ -66,6 +66,26 @@ def test_ntt_large(glc, oracle, log_n, inverse, log_ext, coset):
     run_case(glc, oracle, log_n, 2 if log_n < 23 else 1, inverse, log_ext, coset, seed=log_n * 131 + inverse)
 
 
+@pytest.mark.parametrize("log_n", [5, 13, 18])
+@pytest.mark.parametrize("bitrev_inputs,inverse,log_ext,coset", [(False, False, 1, 1), (False, True, 0, 0),
+                                                                 (True, False, 2, 3), (False, False, 0, 0)])
+def test_odd_stride_and_offset(glc, oracle, log_n, bitrev_inputs, inverse, log_ext, coset):
+    # an odd element offset and an odd stride: the 16-byte load/store path does not apply, the
+    # 8-byte one runs (and must agree)
+    n = 1 << log_n
+    num, off, stride = 3, 1, n + 3
+    x = rand_elems(num * stride, log_n + 7 * coset, noncanonical=True)
+    d_in, d_out = to_dev(x), zeros_dev(num * stride)
+    glc.ntt.batch_ntt_out_of_place(d_in, d_out, log_n, num, off, off, stride, stride, bitrev_inputs, inverse,
+                                   log_ext, coset)
+    got = from_dev(d_out)
+    for k in range(num):
+        sl = slice(k * stride + off, k * stride + off + n)
+        col = np.ascontiguousarray(x[sl])
+        want = oracle.batch_ntt(col, log_n, 1, n, n, int(bitrev_inputs), int(inverse), log_ext, coset)
+        assert (canon(got[sl]) == want).all(), (log_n, k)
+
+
 def test_lde_cosets_every_index(glc, oracle):
     log_n, log_ext = 10, 2
     n = 1 << log_n
