@@ -37,7 +37,11 @@ def check_job(oracle, job, ev):
 
 
 @pytest.mark.parametrize("log_n,cols,log_lde,log_cap", [(12, 8, 1, 4), (13, 9, 2, 4), (16, 16, 1, 4), (5, 3, 2, 2),
-                                                         (14, 24, 0, 0), (10, 130, 1, 1)])
+                                                         (14, 24, 0, 0), (10, 130, 1, 1),
+                                                         # edges: one row pair, one column, the cap is
+                                                         # the whole leaf layer (no node layer), LDE x16
+                                                         (1, 1, 0, 0), (1, 3, 1, 2), (3, 1, 4, 4), (6, 17, 3, 9),
+                                                         (11, 1, 4, 6)])
 def test_commit_plain(glc, oracle, syn, log_n, cols, log_lde, log_cap):
     job, ev = make_job(glc, syn, log_n, cols, log_lde, log_cap, "plain-%d-%d" % (log_n, cols))
     glc.commit.commit(job)
