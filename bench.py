@@ -45,6 +45,17 @@ def job_units(log_n=LOG_N, cols=COLS, log_lde=LOG_LDE, log_cap=LOG_CAP):
             "modmul": modmul}
 
 
+def stage_units(log_n=LOG_N, cols=COLS, log_lde=LOG_LDE, log_cap=LOG_CAP):
+    """Algorithmic modmuls and bytes per stage of one commitment (the split of job_units)."""
+    n, f = 1 << log_n, 1 << log_lde
+    return {
+        "monomials": {"modmul": cols * (n // 2 * log_n + n), "bytes": 32 * n * cols},  # iNTT + bit reversal
+        "ntt": {"modmul": f * cols * (n + n // 2 * log_n), "bytes": 16 * f * n * cols},
+        "leaves": {"modmul": MODMUL_PER_PERM * f * n * ((cols + 7) // 8), "bytes": f * (8 * n * cols + 32 * n)},
+        "nodes": {"modmul": MODMUL_PER_PERM * (f * n - (1 << log_cap)), "bytes": 64 * f * n},
+    }
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -387,6 +398,12 @@ def run_ours(args, rank, world, local_rank):
         "hashes_per_s": (units["perms_leaves"] + units["perms_nodes"]) * world / (ms / 1e3),
         "algorithmic_gbs": units["bytes"] * world / (ms / 1e3) / 1e9,
         "stages_ms": {k: v / args.steps for k, v in stage.items()},
+        # per stage: algorithmic work, its roofline time, and that over the stage's in-step time
+        # (the coset stages run on two streams at once, so their in-step times overlap)
+        "stages_roofline": {k: dict(u, roof_ms=max(u["bytes"] / (peaks["hbm_gbs"] * 1e9), u["modmul"] / mm_peak) * 1e3,
+                                    frac=max(u["bytes"] / (peaks["hbm_gbs"] * 1e9), u["modmul"] / mm_peak) * 1e3
+                                    / max(1e-9, stage[k] / args.steps))
+                            for k, u in stage_units().items()},
         "roofline": {"bound": "int", "kernel": "p2_leaves_kernel", "achieved": achieved,
                      "peak": mm_peak / 1e9, "unit": "Gmodmul/s", "frac": achieved * 1e9 / mm_peak,
                      "launch_ms_in_step": leaf_ms, "launch_ms_alone": leaf_alone_ms,
