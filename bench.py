@@ -674,6 +674,46 @@ def run_ef(args):
     ctx.destroy()
 
 
+def run_queries(args):
+    """Query openings on the headline commitment (128 columns x 2^20 rows, LDE x2, cap 16): for
+    100 seeded query indexes of one coset, gather the 100 rows of the 128 LDE columns
+    (gather_rows) and the 17-layer Merkle paths of the 2^20-leaf subtree (gather_merkle_paths)."""
+    import numpy as np
+    glc, torch, ctx = _setup_device()
+    syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
+    n = 1 << LOG_N
+    sz = glc.CommitJob.sizes(LOG_N, COLS, LOG_LDE, LOG_CAP)
+    dev = lambda k: torch.empty(sz[k], dtype=torch.int64, device="cuda")
+    jb = glc.CommitJob(evals=dev("evals"), log_n=LOG_N, cols=COLS, log_lde=LOG_LDE, log_cap=LOG_CAP, lde=dev("lde"),
+                       trees=dev("trees"), cap=dev("cap"))
+    syn.fill_device(jb.evals, "queries")
+    glc.commit.commit(jb)
+    q = 100
+    idx = torch.from_numpy(np.random.default_rng(5).integers(0, n, q).astype(np.int32)).cuda()
+    layers = LOG_N - (LOG_CAP - LOG_LDE)
+    rows = torch.empty(q * COLS, dtype=torch.int64, device="cuda")
+    paths = torch.empty(layers * 4 * q, dtype=torch.int64, device="cuda")
+    lde0, tree0 = jb.lde[:COLS * n], jb.trees[:8 * n]
+    calls = {"gather_rows": lambda: glc.GLHasher.gather_rows(idx, 0, lde0, n, COLS, rows, q, COLS),
+             "gather_merkle_paths": lambda: glc.GLHasher.gather_merkle_paths(idx, tree0, paths, layers)}
+    out = {"workload": "query openings: 100 indexes, 128 columns x 2^20 rows, 17-layer paths (cap 16 over 2 cosets)"}
+    for name, fn in calls.items():
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        reps = 200
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        us = e0.elapsed_time(e1) / reps * 1e3
+        out[name] = {"us_per_call": us, "queries_per_s": q / (us / 1e6)}
+    print(json.dumps(out), flush=True)
+    ctx.destroy()
+
+
 def run_profile_case(args):
     """A small commitment for profiler captures: 128 columns x 2^log_n rows (default 2^18, 256 MiB of
     inputs, still larger than L2), LDE x2, cap 16; warm-up plus a few plain glc_commit calls."""
@@ -707,7 +747,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-ref-kernels", action="store_true")
-    ap.add_argument("--workload", default="commit", choices=["commit", "uneven", "large", "serve", "profile", "ef"],
+    ap.add_argument("--workload", default="commit", choices=["commit", "uneven", "large", "serve", "profile", "ef", "queries"],
                     help="commit: the contract line; others print their own JSON")
     ap.add_argument("--log-n", type=int, default=18, help="rows of the profile case (log2)")
     ap.add_argument("--ef-log-rows", type=int, default=22, help="rows of the extension-layout workload (log2)")
@@ -719,7 +759,7 @@ def main():
     args = ap.parse_args()
     if args.workload != "commit":
         {"uneven": run_uneven, "large": run_large, "serve": run_serve,
-         "profile": run_profile_case, "ef": run_ef}[args.workload](args)
+         "profile": run_profile_case, "ef": run_ef, "queries": run_queries}[args.workload](args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
