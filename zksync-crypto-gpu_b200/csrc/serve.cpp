@@ -5,6 +5,9 @@
 //
 // Device memory is stream-ordered (cudaMallocAsync / cudaFreeAsync from the device's default
 // memory pool, kept cached between requests), so admission costs no device synchronisation.
+// The streams carry CUDA stream priorities by request size: a small request's blocks are
+// scheduled ahead of the remaining blocks of a large one as SMs free up, so its latency does not
+// include the large request's kernels (unless flat_priority is set).
 #include <cuda_runtime.h>
 
 #include <algorithm>
