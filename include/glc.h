@@ -224,7 +224,9 @@ glc_status glc_server_destroy(glc_server *server);
 /* ---------------------------------------------------------------------------------------------
  * Launch tuning (no counterpart in boojum-cuda, whose plans are fixed tables, ntt.rs:70-169).
  * Values are per device; glc_autotune times candidates on the current device and installs the
- * fastest per NTT size and for the leaf kernel.
+ * fastest per NTT size and for the leaf kernel.  Launches read the values without a lock: set
+ * them (or autotune) before other host threads launch work on that device.  Every choice
+ * computes the same bits.
  */
 typedef struct glc_ntt_tuning {
   uint32_t radix_bits;       /* stages per register round: 2, 3 or 4 */
