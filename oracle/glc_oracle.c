@@ -17,37 +17,48 @@ typedef unsigned __int128 u128;
  * Field.  p = 2^64 - 2^32 + 1.  (crates/boojum-cuda/native/goldilocks.cuh:90-185: the
  * reference keeps values in [0, 2^64) and compares canonically; the oracle canonicalises.)
  * ---------------------------------------------------------------------------------------- */
-uint64_t or_canon(uint64_t a) { return a >= OR_P ? a - OR_P : a; }
+/* Branch-free helpers (the carries are data-dependent, so branches would mispredict half the
+ * time).  fr_* results are in [0, 2^64), congruent mod p but not necessarily canonical. */
+static inline uint64_t fr_canon(uint64_t a) { return a >= OR_P ? a - OR_P : a; }
 
-/* Branch-free (the carries are data-dependent, so branches would mispredict half the time). */
-uint64_t or_add(uint64_t a, uint64_t b) {
-  a = or_canon(a);
-  b = or_canon(b);
-  const uint64_t s = a + b; /* both < p: a carry means s + 2^64 >= p */
-  const uint64_t t = s - OR_P;
-  const int use_t = (s < a) | (s >= OR_P);
-  return use_t ? t : s;
+/* a + b: a carry out of 64 bits is worth EPS = 2^32 - 1; adding it can carry once more only
+ * when the wrapped sum is >= p, and then the second EPS cannot carry (the wrapped sum is at most
+ * 2^64 - 2). */
+static inline uint64_t fr_add(uint64_t a, uint64_t b) {
+  uint64_t s, s2;
+  const uint64_t c1 = __builtin_add_overflow(a, b, &s);
+  const uint64_t c2 = __builtin_add_overflow(s, 0xFFFFFFFFull & (0 - c1), &s2);
+  return s2 + (0xFFFFFFFFull & (0 - c2));
 }
 
+/* 128-bit product reduced with 2^64 = 2^32 - 1 and 2^96 = -1 (mod p): with hi = hh:hl,
+ * x = lo - hh + hl * (2^32 - 1).  A borrow in lo - hh leaves at least 2^64 - 2^32 + 1, so
+ * subtracting EPS for it cannot borrow again; a carry in the final sum leaves less than
+ * (2^32 - 1)^2, so adding EPS for it cannot carry again. */
+static inline uint64_t fr_mul(uint64_t a, uint64_t b) {
+  const u128 x = (u128)a * b;
+  const uint64_t lo = (uint64_t)x, hi = (uint64_t)(x >> 64);
+  const uint64_t hh = hi >> 32, hl = hi & 0xFFFFFFFFull;
+  uint64_t t0, t2;
+  const uint64_t br = __builtin_sub_overflow(lo, hh, &t0);
+  t0 -= 0xFFFFFFFFull & (0 - br);
+  const uint64_t t1 = hl * 0xFFFFFFFFull;
+  const uint64_t cr = __builtin_add_overflow(t0, t1, &t2);
+  return t2 + (0xFFFFFFFFull & (0 - cr));
+}
+
+uint64_t or_canon(uint64_t a) { return fr_canon(a); }
+
+uint64_t or_add(uint64_t a, uint64_t b) { return fr_canon(fr_add(a, b)); }
+
 uint64_t or_sub(uint64_t a, uint64_t b) {
-  a = or_canon(a);
-  b = or_canon(b);
+  a = fr_canon(a);
+  b = fr_canon(b);
   const uint64_t d = a - b;
   return a >= b ? d : d + OR_P;
 }
 
-/* 128-bit product reduced with 2^64 = 2^32 - 1 and 2^96 = -1 (mod p). */
-uint64_t or_mul(uint64_t a, uint64_t b) {
-  u128 x = (u128)a * b;
-  uint64_t lo = (uint64_t)x, hi = (uint64_t)(x >> 64);
-  uint64_t hh = hi >> 32, hl = hi & 0xFFFFFFFFull;
-  uint64_t t0 = lo - hh;
-  if (lo < hh) t0 -= 0xFFFFFFFFull; /* borrow: -2^64 = -(2^32 - 1) */
-  uint64_t t1 = hl * 0xFFFFFFFFull;
-  uint64_t t2 = t0 + t1;
-  if (t2 < t1) t2 += 0xFFFFFFFFull; /* carry: 2^64 = 2^32 - 1 */
-  return or_canon(t2);
-}
+uint64_t or_mul(uint64_t a, uint64_t b) { return fr_canon(fr_mul(a, b)); }
 
 uint64_t or_pow(uint64_t a, uint64_t e) {
   uint64_t r = 1, x = or_canon(a);
@@ -288,14 +299,14 @@ void or_p2_set_round_constants(const uint64_t rc[30 * 12]) { memcpy(g_rc, rc, si
 
 /* m4 from eprint 2023/323 Appendix B (poseidon2_gl.cuh:11-25). */
 static void or_m4(uint64_t *x) {
-  uint64_t t0 = or_add(x[0], x[1]);
-  uint64_t t1 = or_add(x[2], x[3]);
-  uint64_t t2 = or_add(or_add(x[1], x[1]), t1);
-  uint64_t t3 = or_add(or_add(x[3], x[3]), t0);
-  uint64_t t4 = or_add(or_mul(t1, 4), t3);
-  uint64_t t5 = or_add(or_mul(t0, 4), t2);
-  uint64_t t6 = or_add(t3, t5);
-  uint64_t t7 = or_add(t2, t4);
+  uint64_t t0 = fr_add(x[0], x[1]);
+  uint64_t t1 = fr_add(x[2], x[3]);
+  uint64_t t2 = fr_add(fr_add(x[1], x[1]), t1);
+  uint64_t t3 = fr_add(fr_add(x[3], x[3]), t0);
+  uint64_t t4 = fr_add(fr_mul(t1, 4), t3);
+  uint64_t t5 = fr_add(fr_mul(t0, 4), t2);
+  uint64_t t6 = fr_add(t3, t5);
+  uint64_t t7 = fr_add(t2, t4);
   x[0] = t6;
   x[1] = t5;
   x[2] = t7;
@@ -306,35 +317,36 @@ static void or_m4(uint64_t *x) {
 static void or_external(uint64_t *s) {
   for (int t = 0; t < 12; t += 4) or_m4(s + t);
   for (int j = 0; j < 4; j++) {
-    uint64_t acc = or_add(or_add(s[j], s[4 + j]), s[8 + j]);
-    for (int t = 0; t < 12; t += 4) s[t + j] = or_add(s[t + j], acc);
+    uint64_t acc = fr_add(fr_add(s[j], s[4 + j]), s[8 + j]);
+    for (int t = 0; t < 12; t += 4) s[t + j] = fr_add(s[t + j], acc);
   }
 }
 
 /* M_I = J + diag(2^LOG_MU_MINUS_ONE) (poseidon2_gl_st.cuh:57-65). */
 static void or_internal(uint64_t *s) {
   uint64_t sum = 0;
-  for (int i = 0; i < 12; i++) sum = or_add(sum, s[i]);
-  for (int i = 0; i < 12; i++) s[i] = or_add(sum, or_mul(s[i], 1ull << OR_LOG_MU_MINUS_ONE[i]));
+  for (int i = 0; i < 12; i++) sum = fr_add(sum, s[i]);
+  for (int i = 0; i < 12; i++) s[i] = fr_add(sum, fr_mul(s[i], 1ull << OR_LOG_MU_MINUS_ONE[i]));
 }
 
 static uint64_t or_sbox(uint64_t x) {
-  uint64_t x2 = or_mul(x, x), x3 = or_mul(x2, x), x4 = or_mul(x2, x2);
-  return or_mul(x3, x4);
+  uint64_t x2 = fr_mul(x, x), x3 = fr_mul(x2, x), x4 = fr_mul(x2, x2);
+  return fr_mul(x3, x4);
 }
 
+/* Values stay in [0, 2^64) between the rounds and are canonicalised at the end. */
 void or_p2_permutation(uint64_t s[12]) {
-  for (int i = 0; i < 12; i++) s[i] = or_canon(s[i]);
   or_external(s);
   for (int r = 0; r < 30; r++) {
     if (r < 4 || r >= 26) {
-      for (int i = 0; i < 12; i++) s[i] = or_sbox(or_add(s[i], g_rc[r][i]));
+      for (int i = 0; i < 12; i++) s[i] = or_sbox(fr_add(s[i], g_rc[r][i]));
       or_external(s);
     } else {
-      s[0] = or_sbox(or_add(s[0], g_rc[r][0]));
+      s[0] = or_sbox(fr_add(s[0], g_rc[r][0]));
       or_internal(s);
     }
   }
+  for (int i = 0; i < 12; i++) s[i] = fr_canon(s[i]);
 }
 
 typedef struct {
