@@ -149,3 +149,17 @@ def test_device_random_matches_python(glc, syn, count, offset):
     d = zeros_dev(count)
     syn.fill_device(d, "fill-seed", offset)
     assert (from_dev(d) == syn.random_field_elements("fill-seed", count, offset)).all()
+
+
+def test_commit_random_shapes(glc, oracle, syn):
+    # seeded random shapes across the contract: every output equals the oracle's
+    rng = np.random.default_rng(2024)
+    for t in range(10):
+        log_n = int(rng.integers(1, 15))
+        cols = int(rng.integers(1, 41))
+        log_lde = int(rng.integers(0, 4))
+        log_cap = int(rng.integers(log_lde, log_lde + log_n + 1))
+        job, ev = make_job(glc, syn, log_n, cols, log_lde, log_cap, "random-%d" % t,
+                           keep_monomials=bool(rng.integers(0, 2)))
+        glc.commit.commit(job)
+        check_job(oracle, job, ev)
