@@ -44,3 +44,30 @@ def test_contract_checks_without_a_device():
     assert L.glc_poseidon2_compute_node_hashes(None, 16, None, 4, None) == 1
     assert L.glc_bit_reverse(None, 8, None, 8, 6, 1, None) == 1  # rows not a power of two
     assert L.glc_tuning_set_p2(None) == 1
+
+
+def test_header_compiles_as_c_and_links(tmp_path):
+    # a C11 caller (the Rust FFI and cgo-style bindings see the same declarations) compiles
+    # against include/glc.h, links libglc.so and gets a contract violation back without a device
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        import pytest
+        pytest.skip("no C compiler")
+    g = load_package()
+    src = tmp_path / "caller.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <string.h>\n#include "glc.h"\n'
+        "int main(void) {\n"
+        "  glc_status s = glc_batch_ntt_in_place(NULL, 64, 0, 1, 0, 64, false, false, 0, 0, NULL);\n"
+        '  if (s != 1 || !strstr(glc_last_error_message(), "log_n")) return 1;\n'
+        '  printf("ok\\n");\n  return 0;\n}\n')
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(g.LIB_PATH)
+    r = subprocess.run([cc, "-std=c11", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        str(src), "-o", str(exe), "-L", libdir, "-lglc", "-Wl,-rpath," + libdir],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout, r.stderr)
