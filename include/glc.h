@@ -161,7 +161,10 @@ glc_status glc_commit_profiled(const glc_commit_job *job, void *stream, void **e
  * evals, stride, sizes and cap ([4][2^log_cap], device) mean what they mean in glc_commit_job.
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress), so make
  * it before any stream capture on that device.  Calls share the array: calls that overlap on the
- * GPU race; calls ordered on one stream or by events do not.  Needs glc_context_create. */
+ * GPU race; calls ordered on one stream or by events do not.  Needs glc_context_create; the
+ * digests use the round constants installed by glc_poseidon2_set_round_constants (otherwise the
+ * built-in placeholder set).  glc_context_destroy forgets the looked-up address, so after a
+ * device reset create the context again and the next call looks it up anew. */
 glc_status glc_commit_cap_noalloc(const uint64_t *evals, uint64_t evals_stride, uint32_t log_n, uint32_t cols,
                                   uint32_t log_lde, uint32_t log_cap, uint64_t *cap, void *stream);
 
@@ -239,7 +242,8 @@ typedef struct glc_p2_tuning {
   uint32_t leaf_threads; /* 64, 128 or 256 (leaf and wide node-layer kernels) */
   uint32_t rolled;       /* 0: fully unrolled, 1: partial rounds in a loop, 2: full rounds too */
   uint32_t lazy;         /* 1: partial rounds keep 11 of 12 state words partially reduced */
-  uint32_t min_blocks;   /* leaf kernel register cap: 2 -> 128 registers, 3 -> 80 registers */
+  uint32_t min_blocks;   /* leaf kernel register cap: 2 -> 128 registers, 3 -> 85 registers,
+                            5 -> 102 registers (leaf_threads <= 128) */
 } glc_p2_tuning;
 glc_status glc_tuning_get_ntt(uint32_t log_n, glc_ntt_tuning *out);
 glc_status glc_tuning_set_ntt(uint32_t log_n, const glc_ntt_tuning *tuning);

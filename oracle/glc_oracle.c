@@ -485,8 +485,8 @@ static int64_t or_climb(const uint64_t d[4], const uint64_t *path, uint32_t leve
   if (level == depth) {
     for (uint32_t k = 0; k < cap_len; k++)
       if (d[0] == or_canon(cap[4 * k]) && d[1] == or_canon(cap[4 * k + 1]) && d[2] == or_canon(cap[4 * k + 2]) &&
-          d[3] == or_canon(cap[4 * k + 3]) && (index >> depth) == k)
-        return (int64_t)index;
+          d[3] == or_canon(cap[4 * k + 3]))
+        return (int64_t)(index | ((uint64_t)k << depth));
     return -1;
   }
   for (int side = 0; side < 2; side++) {

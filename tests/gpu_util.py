@@ -21,3 +21,18 @@ def zeros_dev(n):
 def from_dev(t):
     torch().cuda.synchronize()
     return t.cpu().numpy().view(np.uint64)
+
+
+class _RawDevice:
+    """A raw device address seen through __cuda_array_interface__ (int64 elements)."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": "<i8", "data": (int(ptr), False),
+                                         "version": 3}
+
+
+def raw_to_host(ptr, n):
+    """Copies n u64 elements from a raw device address (e.g. a resident serving buffer) to numpy."""
+    T = torch()
+    T.cuda.synchronize()
+    return T.as_tensor(_RawDevice(ptr, n), device="cuda").cpu().numpy().view(np.uint64)

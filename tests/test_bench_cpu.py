@@ -36,3 +36,12 @@ def test_reference_arm_two_ranks():
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _lines(r.stdout)
     assert len(lines) == 1 and lines[0]["n_gpus"] == 2
+
+
+def test_reference_arm_loads_no_product_library():
+    """The CPU reference arm maps the oracle only: the product's libglc.so stays unloaded."""
+    code = ("import sys; sys.path.insert(0, %r); import bench; bench.cpu_baseline((8, 4, 1, 2)); "
+            "maps = open('/proc/self/maps').read(); "
+            "sys.exit(2 if 'libglc.so' in maps else (0 if 'libglc_oracle.so' in maps else 3))" % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stderr[-2000:])

@@ -117,7 +117,7 @@ def test_ntt_tuning_invariance(glc, oracle, radix, k1, lw, cpc, mb):
 
 @pytest.mark.parametrize("threads,rolled,lazy,minb", [(64, 0, 0, 2), (128, 1, 1, 3), (256, 0, 1, 2), (256, 1, 0, 3),
                                                      (128, 0, 0, 3), (256, 1, 1, 2), (256, 2, 1, 3), (128, 2, 0, 2),
-                                                     (64, 2, 1, 2), (256, 2, 0, 3)])
+                                                     (64, 2, 1, 2), (256, 2, 0, 3), (128, 2, 1, 5), (64, 1, 0, 5)])
 def test_leaf_tuning_invariance(glc, oracle, threads, rolled, lazy, minb):
     saved = glc.tuning.get_p2()
     glc.tuning.set_p2(threads, rolled, lazy, minb)

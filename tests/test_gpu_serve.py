@@ -78,19 +78,45 @@ def test_rejections_and_cancel(glc):
 
 
 def test_wait_timeout_and_resident(glc, oracle):
-    import torch
+    """A zero-timeout wait either returns the finished request or reports cudaErrorNotReady; the
+    LDE and trees kept resident on the device equal the oracle's either way."""
+    from gpu_util import raw_to_host
+    log_n, cols, log_lde, log_cap = 16, 128, 1, 4
+    ev = inp(3, log_n, cols)
     with glc.serve.Server(hbm_budget_bytes=4 << 30, max_inflight=2, streams=2) as srv:
-        t = srv.submit(inp(3, 16, 128), 16, 128, 1, 4, keep_resident=True)
+        t = srv.submit(ev, log_n, cols, log_lde, log_cap, keep_resident=True)
         try:
-            srv.wait(t, timeout_s=0.0)
-            done_early = True
+            cap, r = srv.wait(t, timeout_s=0.0)  # already finished
         except glc.GlcError as e:
             assert e.status == 600  # cudaErrorNotReady: still running
-            done_early = False
-        if not done_early:
             cap, r = srv.wait(t)
-        else:
-            cap, r = None, None
-        if r is not None:
-            assert r.device_lde
-            srv.release(t)
+        assert r.device_lde and r.device_trees
+        n, f = 1 << log_n, 1 << log_lde
+        _, lde, trees, want_cap = oracle.commit(ev, log_n, cols, log_lde, log_cap)
+        assert (canon(cap) == want_cap).all(), "cap"
+        assert (canon(raw_to_host(r.device_lde, f * cols * n)) == lde).all(), "resident LDE"
+        assert (canon(raw_to_host(r.device_trees, f * 8 * n)) == trees).all(), "resident trees"
+        srv.release(t)
+
+
+def test_submit_does_not_wait_for_copies(glc):
+    """submit() returns within milliseconds while the worker copies a large request's pageable
+    input to the device (2 GiB: that copy takes about 100 ms or more); the small requests
+    submitted meanwhile still finish."""
+    import time
+    log_n, cols = 23, 32
+    big = np.full(cols << log_n, 3, dtype=np.uint64)  # pageable, pages touched
+    small = [inp(10 + i, 12, 8) for i in range(8)]
+    with glc.serve.Server(hbm_budget_bytes=32 << 30, max_inflight=4, streams=2) as srv:
+        t_big = srv.submit(big, log_n, cols, 1, 4)
+        time.sleep(0.02)  # the worker admits it and starts the copy
+        took, tickets = [], []
+        for x in small:
+            t0 = time.perf_counter()
+            tickets.append(srv.submit(x, 12, 8, 1, 4))
+            took.append(time.perf_counter() - t0)
+            time.sleep(0.005)
+        srv.wait(t_big)
+        for t in tickets:
+            srv.wait(t)
+    assert max(took) < 0.02, "submit waited %.1f ms" % (max(took) * 1e3)

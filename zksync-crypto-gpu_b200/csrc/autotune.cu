@@ -63,7 +63,9 @@ extern "C" glc_status glc_tuning_get_p2(glc_p2_tuning *out) {
 extern "C" glc_status glc_tuning_set_p2(const glc_p2_tuning *in) {
   if (!in || (in->leaf_threads != 64 && in->leaf_threads != 128 && in->leaf_threads != 256))
     return fail("tuning: leaf_threads must be 64, 128 or 256");
-  if (in->min_blocks != 2 && in->min_blocks != 3) return fail("tuning: min_blocks must be 2 or 3");
+  if (in->min_blocks != 2 && in->min_blocks != 3 && in->min_blocks != 5)
+    return fail("tuning: min_blocks must be 2, 3 or 5");
+  if (in->min_blocks == 5 && in->leaf_threads > 128) return fail("tuning: min_blocks 5 needs leaf_threads <= 128");
   if (in->rolled > 2) return fail("tuning: rolled must be 0, 1 or 2");
   P2Tuning &t = p2_tuning();
   t.leaf_threads = in->leaf_threads;
@@ -143,8 +145,8 @@ extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint3
     for (uint32_t th : {128u, 256u})
       for (uint32_t rolled : {0u, 1u, 2u})
         for (bool lazy : {false, true})
-          for (uint32_t minb : {2u, 3u}) {
-        if (err) continue;
+          for (uint32_t minb : {2u, 3u, 5u}) {
+        if (err || (minb == 5 && th > 128)) continue;
         P2Tuning c;
         c.leaf_threads = th;
         c.rolled = rolled;

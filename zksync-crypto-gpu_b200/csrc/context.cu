@@ -136,5 +136,6 @@ extern "C" glc_status glc_context_destroy(void) {
   std::lock_guard<std::mutex> lock(g_tables_mutex);
   // cudaFree synchronises the device, so no kernel still reads the tables
   free_tables(g_tables[dev]);
+  noalloc_forget_device(dev);
   return 0;
 }

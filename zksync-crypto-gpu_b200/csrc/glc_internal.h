@@ -63,7 +63,7 @@ struct P2Tuning {
   uint32_t leaf_threads = 128;  // 64, 128 or 256
   uint32_t rolled = 2;          // 0: every round unrolled; 1: partial rounds in a loop; 2: all rounds in loops
   bool lazy = true;             // partial rounds keep s1..s11 partially reduced
-  uint32_t min_blocks = 2;      // leaf kernel register cap: 2 -> 128 registers, 3 -> 80 registers
+  uint32_t min_blocks = 2;      // leaf kernel register cap: 2 -> 128, 3 -> 85, 5 -> 102 registers (<= 128 threads)
 };
 P2Tuning &p2_tuning();
 
@@ -85,6 +85,7 @@ int p2_nodes_launch(const uint64_t *values, uint64_t *results, uint64_t count, c
 int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cudaStream_t stream);
 
 int ntt_init_device();  // kernel attributes; called by glc_context_create
+void noalloc_forget_device(int dev);  // drops the cached scratch address; called by glc_context_destroy
 double job_cost(const glc_commit_job &j);
 int commit_check(const glc_commit_job &j);
 // Enqueues one job; when `events` is given, records events[0] before the first stage, one after

@@ -37,8 +37,17 @@ static __device__ __align__(256) uint64_t g_noalloc_scratch[NOALLOC_ELEMS];
 static uint64_t *g_noalloc_ptr[MAX_DEVICES] = {};
 static std::mutex g_noalloc_mu;
 
+// Forgets the device address looked up on `dev`.  glc_context_destroy calls it: after a device
+// reset (cudaDeviceReset) the caller has to create the context again, and the next call then
+// looks the address up again instead of using one from the old context.
+void noalloc_forget_device(int dev) {
+  if (dev < 0 || dev >= MAX_DEVICES) return;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  g_noalloc_ptr[dev] = nullptr;
+}
+
 // Device address of the array on the current device, looked up once per device (on the first
-// call there) with that device current.
+// call there after glc_context_create) with that device current.
 static int noalloc_scratch(uint64_t **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

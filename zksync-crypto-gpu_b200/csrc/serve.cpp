@@ -3,11 +3,19 @@
 // (continuous batching: a request that arrives while others run starts as soon as memory and a
 // slot free up, and its kernels overlap theirs), and reports per-request latency.
 //
-// Device memory is stream-ordered (cudaMallocAsync / cudaFreeAsync from the device's default
-// memory pool, kept cached between requests), so admission costs no device synchronisation.
+// Device memory is stream-ordered (cudaMallocFromPoolAsync / cudaFreeAsync from a memory pool
+// private to the server, which keeps freed blocks cached between requests), so admission costs
+// no device synchronisation and the device's default pool keeps its settings.
 // The streams carry CUDA stream priorities by request size: a small request's blocks are
 // scheduled ahead of the remaining blocks of a large one as SMs free up, so its latency does not
 // include the large request's kernels (unless flat_priority is set).
+//
+// Locking: the server mutex guards the queues, the request table and the counters only.  The
+// worker decides admissions and completions under it, then releases it for the CUDA calls that
+// can block the host (a host-to-device copy from pageable memory runs synchronously, the cap
+// copy waits for its stream), so submit, wait and stats never wait behind a copy.  A request
+// that is started and not yet done belongs to the worker: nothing else erases it from the table
+// (std::map keeps the addresses of its other entries stable).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -49,6 +57,7 @@ struct Server {
   std::vector<uint32_t> stream_class;  // 0 = highest priority
   uint32_t classes = 1;
   cudaStream_t copy_stream = nullptr;  // result copies to the host
+  cudaMemPool_t pool = nullptr;        // private stream-ordered pool (release threshold: never)
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<uint64_t> pending;
@@ -89,10 +98,8 @@ static uint32_t request_class(const Server &s, uint64_t footprint) {
   return c;
 }
 
-// Allocates and enqueues one admitted request (worker thread, lock held by the caller).
-static int start_request(Server &s, Request &q) {
-  const glc_serve_request &r = q.req;
-  const uint64_t n = 1ull << r.log_n, f = 1ull << r.log_lde;
+// Picks the stream of an admitted request (worker thread, lock held by the caller).
+static void assign_stream(Server &s, Request &q) {
   // least-loaded stream of the request's priority class (any stream when none has that class)
   const uint32_t cls = request_class(s, q.footprint);
   int best = -1;
@@ -104,10 +111,18 @@ static int start_request(Server &s, Request &q) {
       if (s.stream_load[i] < s.stream_load[best]) best = (int)i;
   }
   q.stream = best;
-  cudaStream_t st = s.streams[best];
+  s.stream_load[best]++;
+}
+
+// Allocates, copies and enqueues one admitted request (worker thread, lock NOT held: the copy
+// from pageable host memory blocks this thread until the data is staged).
+static int start_request(Server &s, Request &q) {
+  const glc_serve_request &r = q.req;
+  const uint64_t n = 1ull << r.log_n, f = 1ull << r.log_lde;
+  cudaStream_t st = s.streams[q.stream];
   cudaError_t e = cudaSuccess;
   auto alloc = [&](uint64_t **p, uint64_t elems) {
-    if (e == cudaSuccess) e = cudaMallocAsync((void **)p, elems * sizeof(uint64_t), st);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)p, elems * sizeof(uint64_t), s.pool, st);
   };
   alloc(&q.d_evals, (uint64_t)r.cols * n);
   alloc(&q.d_lde, f * r.cols * n);
@@ -133,7 +148,6 @@ static int start_request(Server &s, Request &q) {
   // here into pageable memory would block this thread until the whole job had finished
   if (!err) err = (int)cudaEventCreateWithFlags(&q.done_event, cudaEventDisableTiming);
   if (!err) err = (int)cudaEventRecord(q.done_event, st);
-  s.stream_load[best]++;
   return err;
 }
 
@@ -151,11 +165,27 @@ static void free_request(Server &s, Request &q, bool keep_resident) {
   q.done_event = nullptr;
 }
 
+// Copies the cap of a finished request to the host and frees its buffers (worker thread, lock
+// NOT held).  Returns the request's final status.
+static int finish_request(Server &s, Request &q, int status) {
+  if (!status) {
+    cudaError_t ce = cudaMemcpyAsync(q.req.host_cap, q.d_cap, (4ull << q.req.log_cap) * 8, cudaMemcpyDeviceToHost,
+                                     s.copy_stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s.copy_stream);
+    status = (int)ce;
+  }
+  free_request(s, q, q.req.keep_resident && !status);
+  return status;
+}
+
 static void worker_main(Server *s) {
   cudaSetDevice(s->device);
+  std::vector<Request *> admitted, finished;
+  std::vector<int> finished_status;
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
     // admit: FIFO; a request that does not fit lets smaller ones behind it start (backfill)
+    admitted.clear();
     for (auto it = s->pending.begin(); it != s->pending.end() && s->inflight < s->cfg.max_inflight;) {
       Request &q = s->reqs[*it];
       if (q.cancelled) {
@@ -172,34 +202,46 @@ static void worker_main(Server *s) {
       s->inflight++;
       s->peak_bytes = std::max(s->peak_bytes, s->used_bytes);
       s->peak_inflight = std::max(s->peak_inflight, s->inflight);
-      q.status = start_request(*s, q);
+      assign_stream(*s, q);
+      admitted.push_back(&q);
       it = s->pending.erase(it);
     }
-    // completions
+    if (!admitted.empty()) {
+      lk.unlock();
+      for (Request *q : admitted) q->status = start_request(*s, *q);
+      lk.lock();
+    }
+    // completions: decided under the lock, copies and frees outside it
+    finished.clear();
+    finished_status.clear();
     bool any_inflight = false;
     for (auto &kv : s->reqs) {
       Request &q = kv.second;
       if (!q.started || q.done) continue;
       cudaError_t qe = q.status ? cudaSuccess : cudaEventQuery(q.done_event);
       if (q.status || qe != cudaErrorNotReady) {
-        if (!q.status && qe != cudaSuccess) q.status = (int)qe;
-        if (!q.status) {
-          cudaError_t ce = cudaMemcpyAsync(q.req.host_cap, q.d_cap, (4ull << q.req.log_cap) * 8,
-                                           cudaMemcpyDeviceToHost, s->copy_stream);
-          if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->copy_stream);
-          q.status = (int)ce;
-        }
-        q.done = true;
-        q.t_done = now_s();
-        s->stream_load[q.stream]--;
-        free_request(*s, q, q.req.keep_resident && !q.status);
-        if (!(q.req.keep_resident && !q.status)) s->used_bytes -= q.footprint;
-        s->inflight--;
-        s->completed++;
-        s->cv_done.notify_all();
+        finished.push_back(&q);
+        finished_status.push_back(q.status ? q.status : (qe != cudaSuccess ? (int)qe : 0));
       } else {
         any_inflight = true;
       }
+    }
+    if (!finished.empty()) {
+      lk.unlock();
+      for (size_t i = 0; i < finished.size(); i++) finished_status[i] = finish_request(*s, *finished[i], finished_status[i]);
+      lk.lock();
+      for (size_t i = 0; i < finished.size(); i++) {
+        Request &q = *finished[i];
+        q.status = finished_status[i];
+        q.done = true;
+        q.t_done = now_s();
+        s->stream_load[q.stream]--;
+        if (!(q.req.keep_resident && !q.status)) s->used_bytes -= q.footprint;
+        s->inflight--;
+        s->completed++;
+      }
+      s->cv_done.notify_all();
+      continue;  // admissions may fit now
     }
     if (s->stop && s->pending.empty() && !any_inflight) break;
     if (any_inflight)
@@ -226,13 +268,25 @@ extern "C" glc_status glc_server_create(const glc_server_config *config, glc_ser
   s.cfg = *config;
   if (s.cfg.streams == 0) s.cfg.streams = 8;
   cudaGetDevice(&s.device);
-  // keep freed blocks in the pool: requests of similar sizes reuse them without new mappings
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, s.device) == cudaSuccess) {
+  // a private pool that keeps freed blocks: requests of similar sizes reuse them without new
+  // mappings, and the device's default pool (shared with other code in the process) is untouched
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = s.device;
+  cudaError_t pe = cudaMemPoolCreate(&s.pool, &props);
+  if (pe == cudaSuccess) {
     uint64_t threshold = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    pe = cudaMemPoolSetAttribute(s.pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  if (pe != cudaSuccess) {
+    if (s.pool) cudaMemPoolDestroy(s.pool);
+    delete srv;
+    return (int)pe;
   }
   if (cudaStreamCreateWithFlags(&s.copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaMemPoolDestroy(s.pool);
     delete srv;
     return fail("serve: cannot create the copy stream");
   }
@@ -248,6 +302,8 @@ extern "C" glc_status glc_server_create(const glc_server_config *config, glc_ser
                                         : cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
       for (auto x : s.streams) cudaStreamDestroy(x);
+      cudaStreamDestroy(s.copy_stream);
+      cudaMemPoolDestroy(s.pool);
       delete srv;
       return (int)e;
     }
@@ -265,6 +321,7 @@ extern "C" glc_status glc_server_submit(glc_server *srv, const glc_serve_request
   int e = request_check(*req);
   if (e) return e;
   Server &s = srv->s;
+  const double t_submit = now_s();  // before the lock: latency counts any wait for it
   const uint64_t fp = request_footprint(*req);
   std::lock_guard<std::mutex> lk(s.mu);
   if (fp > s.cfg.hbm_budget_bytes) {
@@ -276,7 +333,7 @@ extern "C" glc_status glc_server_submit(glc_server *srv, const glc_serve_request
   q.ticket = s.next_ticket++;
   q.req = *req;
   q.footprint = fp;
-  q.t_submit = now_s();
+  q.t_submit = t_submit;
   s.reqs[q.ticket] = q;
   s.pending.push_back(q.ticket);
   *ticket = q.ticket;
@@ -373,6 +430,7 @@ extern "C" glc_status glc_server_destroy(glc_server *srv) {
     cudaStreamDestroy(st);
   }
   if (s.copy_stream) cudaStreamDestroy(s.copy_stream);
+  if (s.pool) cudaMemPoolDestroy(s.pool);  // every block was freed above (stream-ordered, synchronised)
   delete srv;
   return 0;
 }
