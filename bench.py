@@ -837,6 +837,15 @@ def run_profile_case(args):
     ctx.destroy()
 
 
+def run_probe(args):
+    """The modular-multiply probe alone (the roofline denominator), for instruction-mix captures."""
+    glc, torch, ctx = _setup_device()
+    rate = modmul_probe(glc, torch, torch.cuda.current_stream())
+    print(json.dumps({"workload": "glc_modmul_probe: 148 x 32 blocks x 256 threads, 8 chains x 2048 multiplies",
+                      "Gmodmul_s": rate / 1e9}), flush=True)
+    ctx.destroy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -845,7 +854,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-ref-kernels", action="store_true", help="skip the reference-kernel timing and parity leg")
     ap.add_argument("--no-extras", action="store_true", help="skip the 128 x 2^20 and uneven-batch extra keys")
-    ap.add_argument("--workload", default="commit", choices=["commit", "uneven", "serve", "profile", "ef", "queries"],
+    ap.add_argument("--workload", default="commit",
+                    choices=["commit", "uneven", "serve", "profile", "ef", "queries", "probe"],
                     help="commit: the contract line; others print their own JSON")
     ap.add_argument("--log-n", type=int, default=18, help="rows of the profile case (log2)")
     ap.add_argument("--cols", type=int, default=176, help="columns of the profile case")
@@ -858,7 +868,7 @@ def main():
     args = ap.parse_args()
     if args.workload != "commit":
         {"uneven": run_uneven, "serve": run_serve, "profile": run_profile_case, "ef": run_ef,
-         "queries": run_queries}[args.workload](args)
+         "queries": run_queries, "probe": run_probe}[args.workload](args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

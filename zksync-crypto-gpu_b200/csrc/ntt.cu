@@ -428,8 +428,11 @@ int ntt_launch(const uint64_t *in, uint64_t *out, uint32_t log_n, uint32_t num_n
       a.cols_per_cta = cpc;
       const uint32_t gy = (cols + cpc - 1) / cpc;
       // tile + block twiddles (+ the P/Q scaling tables on a scaled pass)
+      // (the inverse NTT's last pass without a coset multiplies by N^-1 only: no tables, and the
+      // 2^k-entry table it does not need would cost a third CTA per SM on 2^12-element tiles)
+      const bool tables = a.scale == 1 || (a.scale == 2 && a.log_ext);
       const size_t smem = ((size_t(1) << tile_log) + (size_t(1) << ps.k) +
-                           (a.scale ? (size_t(1) << ps.k) + (size_t(1) << ps.log_w) : 0)) *
+                           (tables ? (size_t(1) << ps.k) + (size_t(1) << ps.log_w) : 0)) *
                           sizeof(uint64_t);
       const uint32_t threads =
           (uint32_t)std::min<uint64_t>(pass_threads(tu.radix_bits), std::max<uint64_t>(32, (1ull << tile_log) >> tu.radix_bits));

@@ -121,8 +121,21 @@ static int start_request(Server &s, Request &q) {
   const uint64_t n = 1ull << r.log_n, f = 1ull << r.log_lde;
   cudaStream_t st = s.streams[q.stream];
   cudaError_t e = cudaSuccess;
+  // The pool keeps freed blocks mapped (release threshold: never), so requests of other sizes can
+  // find the device full of cached blocks they cannot use.  On an allocation failure the pool
+  // gives those blocks back (trim) and the allocation is retried; if that is not enough, the
+  // frees still queued on the server's streams are waited for and the pool trimmed again.
   auto alloc = [&](uint64_t **p, uint64_t elems) {
-    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)p, elems * sizeof(uint64_t), s.pool, st);
+    if (e != cudaSuccess) return;
+    const size_t bytes = elems * sizeof(uint64_t);
+    e = cudaMallocFromPoolAsync((void **)p, bytes, s.pool, st);
+    for (int attempt = 0; e == cudaErrorMemoryAllocation && attempt < 2; attempt++) {
+      cudaGetLastError();  // allocation failures are not sticky; clear the record
+      if (attempt == 1)
+        for (cudaStream_t x : s.streams) cudaStreamSynchronize(x);
+      cudaMemPoolTrimTo(s.pool, 0);
+      e = cudaMallocFromPoolAsync((void **)p, bytes, s.pool, st);
+    }
   };
   alloc(&q.d_evals, (uint64_t)r.cols * n);
   alloc(&q.d_lde, f * r.cols * n);
