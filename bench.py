@@ -595,7 +595,8 @@ def uneven_batch(glc, torch, budget_gb=120.0, streams=8, with_reference=True, jo
         used += b
     waves.append(cur)
     stream = torch.cuda.current_stream()
-    t = {"plain": 0.0, "batched": 0.0, "graph": 0.0, "reference_kernels": 0.0}
+    t = {"plain": 0.0, "batched": 0.0, "graph": 0.0, "fused": 0.0, "reference_kernels": 0.0}
+    fused = all(l <= 16 for l, _, _, _ in jobs)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     try:
         import refkern
@@ -622,7 +623,13 @@ def uneven_batch(glc, torch, budget_gb=120.0, streams=8, with_reference=True, jo
         graph.launch()
         torch.cuda.synchronize()
         caps_graph = [jb.cap.clone() for jb in bufs]
-        for form in ("plain", "batched", "graph"):
+        # the fused form (one cooperative launch for every stage of every job) takes waves of
+        # jobs of at most 2^16 rows
+        forms = ("plain", "batched", "graph") + (("fused",) if fused else ())
+        if fused:
+            glc.commit.commit_batch_fused(bufs, stream)
+            torch.cuda.synchronize()
+        for form in forms:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             if form == "plain":
@@ -630,12 +637,14 @@ def uneven_batch(glc, torch, budget_gb=120.0, streams=8, with_reference=True, jo
                     glc.commit.commit(jb, stream)
             elif form == "batched":
                 glc.commit.commit_batch(bufs, n_streams=streams)
-            else:
+            elif form == "graph":
                 graph.launch()
+            else:
+                glc.commit.commit_batch_fused(bufs, stream)
             e1.record()
             torch.cuda.synchronize()
             t[form] += e0.elapsed_time(e1)
-        caps_equal &= all(bool((a == jb.cap).all()) for a, jb in zip(caps_graph, bufs))
+            caps_equal &= all(bool((a == jb.cap).all()) for a, jb in zip(caps_graph, bufs))
         graph.close()
         if have_ref:
             # the reference's own kernels, one call sequence per job (its per-call form)
@@ -679,6 +688,12 @@ def uneven_batch(glc, torch, budget_gb=120.0, streams=8, with_reference=True, jo
                                             "speedup_graph_vs_reference": t["reference_kernels"] / t["graph"]}
                                            if have_ref else None),
             "caps_identical_across_forms": caps_equal, "streams": streams}
+    if fused:
+        line["batched_fused_one_launch"] = {"ms": t["fused"], "value": elements / (t["fused"] / 1e3),
+                                            "speedup_vs_plain": t["plain"] / t["fused"],
+                                            "speedup_vs_graph": t["graph"] / t["fused"],
+                                            "speedup_vs_reference": (t["reference_kernels"] / t["fused"]
+                                                                     if have_ref else None)}
     return line
 
 

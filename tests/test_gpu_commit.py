@@ -72,6 +72,34 @@ def test_commit_batch_uneven_and_alone(glc, oracle, syn):
     assert (from_dev(j0.lde) == from_dev(jobs[1][0].lde)).all()
 
 
+def test_commit_batch_fused(glc, oracle, syn):
+    """The fused batch (one cooperative launch for every stage of every job) on uneven small jobs:
+    1-pass and 2-pass NTT sizes, LDE x1..x16, with and without a monomials buffer, caps from one
+    entry per coset to the whole leaf layer; each equals the oracle's commitment."""
+    shapes = [(12, 8, 1, 4, True), (13, 9, 2, 4, False), (16, 16, 1, 4, True), (5, 3, 2, 2, False),
+              (14, 24, 0, 0, False), (10, 130, 1, 1, True), (1, 1, 0, 0, True), (3, 1, 4, 4, False),
+              (15, 40, 2, 6, False), (12, 64, 3, 5, True), (11, 1, 4, 15, False), (16, 8, 2, 4, False)]
+    jobs = [make_job(glc, syn, l, c, e, cap, "fused-%d" % i, keep_monomials=m)
+            for i, (l, c, e, cap, m) in enumerate(shapes)]
+    glc.commit.commit_batch_fused([j for j, _ in jobs])
+    for j, ev in jobs:
+        check_job(oracle, j, ev)
+    # again on the same buffers (the work table is rebuilt per call), after zeroing the outputs
+    for j, _ in jobs:
+        j.cap.zero_()
+        j.trees.zero_()
+    glc.commit.commit_batch_fused([j for j, _ in jobs])
+    for j, ev in jobs:
+        check_job(oracle, j, ev)
+
+
+def test_commit_batch_fused_contract(glc, syn):
+    job, _ = make_job(glc, syn, 17, 1, 1, 4, "fused-big")
+    with pytest.raises(glc.GlcError):
+        glc.commit.commit_batch_fused([job])
+    glc.commit.commit_batch_fused([])  # nothing to do
+
+
 def test_commit_graph_replay(glc, oracle, syn):
     shapes = [(12, 8, 1), (13, 16, 2), (12, 32, 1)]
     jobs = [make_job(glc, syn, l, c, e, 4, "graph-%d" % i) for i, (l, c, e) in enumerate(shapes)]

@@ -3,7 +3,8 @@
 The sequence shivini runs around boojum-cuda for one commitment
 (crates/shivini/src/data_structures/storage.rs:155-330, cache.rs:353-418), as one call
 (glc_commit), as a batch of uneven jobs on concurrent streams (glc_commit_batch), or as a
-captured CUDA graph replayed with one launch (CommitGraph).
+captured CUDA graph replayed with one launch (CommitGraph), or, for jobs of at most 2^16 rows, as
+one persistent cooperative launch that runs every stage of every job (commit_batch_fused).
 """
 from __future__ import annotations
 
@@ -72,6 +73,13 @@ def commit_batch(jobs: list[CommitJob], n_streams: int = 0, stream=None) -> None
     """Many commitments as one unit on `stream` (glc_commit_batch)."""
     arr = _array(jobs)
     call("glc_commit_batch", C.addressof(arr) if jobs else None, len(jobs), n_streams, stream_handle(stream))
+
+
+def commit_batch_fused(jobs: list[CommitJob], stream=None) -> None:
+    """Many small commitments (2^log_n <= 2^16 rows each) in ONE cooperative launch
+    (glc_commit_batch_fused): every stage of every job, stage by stage, with grid-wide barriers."""
+    arr = _array(jobs)
+    call("glc_commit_batch_fused", C.addressof(arr) if jobs else None, len(jobs), stream_handle(stream))
 
 
 class CommitGraph:

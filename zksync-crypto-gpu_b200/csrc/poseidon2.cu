@@ -302,12 +302,11 @@ __device__ __forceinline__ void permutation(uint64_t s[WIDTH]) {
 // Register cap: MINB = 2 allows 128 registers (two 256-thread CTAs per SM), MINB = 3 allows 85
 // (three 256-thread CTAs), MINB = 5 allows 102 with at most 128 threads per CTA (five CTAs).
 __host__ __device__ constexpr int leaf_max_threads(int minb) { return minb == 5 ? 128 : 256; }
-template <int ROLL, bool LAZY, int MINB>
-__global__ void __launch_bounds__(leaf_max_threads(MINB), MINB) p2_leaves_kernel(const uint64_t *values, uint64_t *results, uint32_t log_rows,
-                                                        uint64_t cols, uint64_t count, bool load_intermediate,
-                                                        bool store_intermediate) {
-  const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= count) return;
+// The leaf hash of leaf gid (one thread's work in p2_leaves_kernel and in the fused batch kernel).
+template <int ROLL, bool LAZY>
+__device__ __forceinline__ void leaf_hash(const uint64_t *values, uint64_t *results, uint32_t log_rows, uint64_t cols,
+                                          uint64_t count, bool load_intermediate, bool store_intermediate,
+                                          uint64_t gid) {
   uint64_t s[WIDTH];
 #pragma unroll
   for (int i = 0; i < WIDTH; i++) s[i] = 0;
@@ -321,7 +320,7 @@ __global__ void __launch_bounds__(leaf_max_threads(MINB), MINB) p2_leaves_kernel
   const uint64_t col_stride = rows * count;
   // value o of this leaf: row o % rows of column o / rows.  The next chunk's 8 values are loaded
   // before the current permutation runs, so the DRAM latency of 8 column streams hides behind
-  // ~15K instructions of hashing.  One permutation call site keeps the code small.
+  // ~14K instructions of hashing.  One permutation call site keeps the code small.
   uint64_t nxt[8];
 #pragma unroll
   for (int i = 0; i < 8; i++)
@@ -340,6 +339,15 @@ __global__ void __launch_bounds__(leaf_max_threads(MINB), MINB) p2_leaves_kernel
   }
 #pragma unroll
   for (int k = 0; k < 4; k++) results[gid + k * count] = canon(store_intermediate ? s[8 + k] : s[k]);
+}
+
+template <int ROLL, bool LAZY, int MINB>
+__global__ void __launch_bounds__(leaf_max_threads(MINB), MINB) p2_leaves_kernel(const uint64_t *values, uint64_t *results, uint32_t log_rows,
+                                                        uint64_t cols, uint64_t count, bool load_intermediate,
+                                                        bool store_intermediate) {
+  const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= count) return;
+  leaf_hash<ROLL, LAZY>(values, results, log_rows, cols, count, load_intermediate, store_intermediate, gid);
 }
 
 // Node hashes (poseidon2_gl_st.cu:61-82): node i = P2(L0..L3, R0..R3, 0,0,0,0)[0..4] with
@@ -732,3 +740,7 @@ extern "C" glc_status glc_poseidon2_gather_merkle_paths(const uint32_t *indexes,
       indexes, (uint32_t)indexes_len, values, log_leaves, results, layers_count);
   return last_launch_error();
 }
+
+// The fused batch of small commitments (one cooperative launch), which uses this file's round
+// constants and hash functions.
+#include "fused.cuh"
