@@ -173,14 +173,19 @@ glc_status glc_commit_cap_noalloc(const uint64_t *evals, uint64_t evals_stride, 
  * Capturable into a CUDA graph. */
 glc_status glc_commit_batch(const glc_commit_job *jobs, uint32_t n_jobs, uint32_t n_streams, void *stream);
 
-/* Many small commitments (log_n <= 16 each) in ONE launch: a persistent cooperative grid runs
- * every stage of every job (inverse NTT, bit reversal, coset NTTs, leaves, node layers, caps),
- * stage by stage with grid-wide barriers, each stage's work items of all jobs spread over the
- * grid.  Same results as glc_commit on each job.  Allocates (stream-ordered) and copies a small
- * work table per call; not for use inside stream capture.  No counterpart in the reference, whose
- * per-call form launches one kernel per NTT stage (log_n < 16) and per tree layer
- * (crates/boojum-cuda/src/ntt.rs:201-241, src/poseidon2.rs:276-295). */
+/* Many small commitments (log_n <= 16 each) in ONE launch: a persistent grid (launched
+ * cooperatively, so all its CTAs are resident) takes work items of every stage of every job
+ * (inverse NTT tiles, bit reversal, coset NTT tiles, leaves, node layers, caps) from a global
+ * counter in stage order; each item waits (bounded, about 1 s) only for the items it reads from,
+ * so different jobs' stages overlap.  Same results as glc_commit on each job.  Allocates
+ * (stream-ordered) and copies a small work table per call; not for use inside stream capture.
+ * No counterpart in the reference, whose per-call form launches one kernel per NTT stage
+ * (log_n < 16) and per tree layer (crates/boojum-cuda/src/ntt.rs:201-241, src/poseidon2.rs:276-295). */
 glc_status glc_commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs, void *stream);
+/* Waits of glc_commit_batch_fused that expired on the current device since the library was
+ * loaded (0 unless something is wrong; a launch with an expired wait computes wrong results).
+ * Synchronous. */
+glc_status glc_commit_batch_fused_timeouts(uint64_t *out);
 
 /* A batch captured once into a CUDA graph and replayed with one launch.  The graph keeps the
  * buffer addresses of the jobs it was created with. */

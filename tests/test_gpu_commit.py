@@ -91,6 +91,26 @@ def test_commit_batch_fused(glc, oracle, syn):
     glc.commit.commit_batch_fused([j for j, _ in jobs])
     for j, ev in jobs:
         check_job(oracle, j, ev)
+    assert glc.commit.fused_timeouts() == 0
+
+
+def test_commit_batch_fused_many_jobs(glc, syn):
+    """80 seeded random small jobs in one launch: every cap equals glc_commit's (the per-call
+    form, itself checked against the oracle), and no dependency wait expired."""
+    rng = np.random.default_rng(77)
+    jobs = []
+    for t in range(80):
+        l = int(rng.integers(8, 17))
+        e = int(rng.integers(0, 3))
+        jobs.append(make_job(glc, syn, l, int(rng.integers(1, 40)), e, int(rng.integers(e, e + 5)), "fmany-%d" % t,
+                             keep_monomials=bool(rng.integers(0, 2)))[0])
+    glc.commit.commit_batch_fused(jobs)
+    got = [from_dev(j.cap).copy() for j in jobs]
+    for j in jobs:
+        glc.commit.commit(j)
+    for j, g in zip(jobs, got):
+        assert (from_dev(j.cap) == g).all(), (j.log_n, j.cols, j.log_lde, j.log_cap)
+    assert glc.commit.fused_timeouts() == 0
 
 
 def test_commit_batch_fused_contract(glc, syn):

@@ -76,10 +76,18 @@ def commit_batch(jobs: list[CommitJob], n_streams: int = 0, stream=None) -> None
 
 
 def commit_batch_fused(jobs: list[CommitJob], stream=None) -> None:
-    """Many small commitments (2^log_n <= 2^16 rows each) in ONE cooperative launch
-    (glc_commit_batch_fused): every stage of every job, stage by stage, with grid-wide barriers."""
+    """Many small commitments (2^log_n <= 2^16 rows each) in ONE persistent launch
+    (glc_commit_batch_fused): work items of every stage of every job, each waiting only for the
+    items it reads from."""
     arr = _array(jobs)
     call("glc_commit_batch_fused", C.addressof(arr) if jobs else None, len(jobs), stream_handle(stream))
+
+
+def fused_timeouts() -> int:
+    """Expired waits of commit_batch_fused on this device since load (0 unless something is wrong)."""
+    v = C.c_uint64()
+    call("glc_commit_batch_fused_timeouts", C.byref(v))
+    return v.value
 
 
 class CommitGraph:

@@ -1,19 +1,26 @@
-// Fused batch of small commitments: ONE cooperative launch runs every stage of every job.
+// Fused batch of small commitments: ONE persistent launch runs every stage of every job.
 //
 // The per-call form issues about 28 kernels per commitment (NTT passes, bit reversal, one leaf
 // launch and node layers per coset, the cap gather); for jobs of 2^12..2^16 rows each of those
 // kernels runs for microseconds and cannot fill 148 SMs, so a batch of such jobs is bound by
 // launch latency and by the tails of small grids (the reference's per-stage and per-layer
 // launches, crates/boojum-cuda/src/ntt.rs:201-241 and src/poseidon2.rs:276-295, are the same
-// shape).  Here a persistent grid (as many CTAs as fit on the device at once) walks a table of
-// work items, stage by stage:
+// shape).  Here a persistent grid (as many CTAs as fit on the device at once, launched
+// cooperatively so that all of them are resident) takes work items from one global counter, in
+// a topological order:
 //   inverse NTT pass 1, pass 2 -> bit reversal -> forward coset NTT pass 1, pass 2 (the coset
-//   that transforms the monomials in place last, in steps of its own) -> leaf hashes -> node
-//   layer 1, 2, ... -> cap gather,
-// with a grid-wide barrier (cooperative groups grid.sync) between steps.  Within a step every
-// work item of every job is independent: an NTT tile, 256 rows of a bit reversal, 256 leaves,
-// 256 nodes, 256 cap entries.  The items reuse the tile and hash code of the per-call kernels
-// (ntt_pass_tile, leaf_hash, hash_node), so the results are the same bits.
+//   that transforms the monomials in place last, after the others have read them) -> leaf
+//   hashes -> node layer 1, 2, ... -> cap gather,
+// every stage listing the items of all jobs, heaviest first.  An item is an NTT tile, 256 rows of
+// a bit reversal, 256 leaves, 256 nodes or 256 cap entries.  Before it runs, an item waits until
+// the items it reads from are done: each stage of each job (per coset where it applies) counts
+// its finished items, and the item waits for its producer's count to reach the producer's item
+// total.  Items wait only for items that come earlier in the order, which some resident CTA
+// fetched already, so the grid always makes progress; different jobs' stages overlap freely.
+// Every wait is bounded (about 1 s): on expiry the item counts a timeout in a device counter
+// (glc_commit_batch_fused_timeouts), raises the launch's abort flag, which ends every other
+// wait, and runs anyway, so a bug shows as wrong results and a non-zero count, never as a hang.  The items reuse the tile and hash code of the per-call
+// kernels (ntt_pass_tile, leaf_hash, hash_node), so the results are the same bits.
 //
 // Included at the end of poseidon2.cu: it needs that file's __constant__ round constants.
 #pragma once
@@ -32,12 +39,17 @@ static constexpr uint32_t FUSED_MAX_LOG_N = 16;
 
 enum FusedKind : uint32_t { FK_NTT = 0, FK_BITREV = 1, FK_LEAVES = 2, FK_NODES = 3, FK_CAPS = 4 };
 
-// One job's share of one step.  Units are numbered across the entries of a step.
+static constexpr uint32_t NO_COUNTER = 0xFFFFFFFFu;
+
+// One job's share of one stage: `units` items, numbered globally from `first`.
 struct FusedEntry {
-  uint64_t first;          // the step's unit number of this entry's first unit
+  uint64_t first;          // global number of this entry's first item
   uint64_t units;
   uint32_t kind;
   uint32_t log_rows;       // bit reversal: log2 of the rows
+  uint32_t dep;            // counter this entry's items wait on (NO_COUNTER: none) ...
+  uint32_t dep_target;     // ... until it reaches this value
+  uint32_t done1, done2;   // counters each finished item increments (NO_COUNTER: none)
   uint64_t tiles_per_col;  // NTT: tiles per column (units = tiles_per_col x column groups)
   PassArgs ntt;            // NTT: the pass
   const uint64_t *src;     // leaves: values; nodes: child layer; caps: trees
@@ -49,90 +61,143 @@ struct FusedEntry {
   uint32_t ccap;           // caps: cap entries per coset
 };
 
-struct FusedStep {
-  uint32_t first_entry, entries;
-  uint64_t units;
-};
+// Waits that expired (device-wide, since the library was loaded).
+static __device__ unsigned long long g_fused_timeouts;
 
-__global__ void __launch_bounds__(FUSED_THREADS, 3) fused_commit_kernel(const FusedEntry *entries, const FusedStep *steps,
-                                                                        uint32_t n_steps) {
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void red_release_add(uint32_t *p, uint32_t v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+static constexpr uint32_t FUSED_WAIT_LIMIT = 1u << 22;  // x 200 ns sleeps: about 1 s
+
+__global__ void __launch_bounds__(FUSED_THREADS, 3)
+    fused_commit_kernel(const FusedEntry *entries, uint32_t n_entries, uint64_t total_units, uint32_t *counters,
+                        uint32_t *abort_flag, unsigned long long *next_unit) {
   extern __shared__ uint64_t smem[];
-  cg::grid_group grid = cg::this_grid();
+  __shared__ uint64_t s_unit;
   const uint32_t tid = threadIdx.x;
-  for (uint32_t st = 0; st < n_steps; st++) {
-    const FusedStep S = steps[st];
-    for (uint64_t u = blockIdx.x; u < S.units; u += gridDim.x) {
-      // the entry holding unit u: the last one whose first unit is <= u (uniform per CTA)
-      uint32_t lo = S.first_entry, hi = S.first_entry + S.entries - 1;
-      while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1) >> 1;
-        if (entries[mid].first <= u)
-          lo = mid;
-        else
-          hi = mid - 1;
-      }
-      const FusedEntry &E = entries[lo];
-      const uint64_t local = u - E.first;
-      const uint32_t kind = E.kind;
-      if (kind == FK_NTT) {
-        const PassArgs a = E.ntt;
-        const uint64_t tpc = E.tiles_per_col;
-        __syncthreads();  // the previous item's last reads of shared memory are done
-        ntt_pass_tile<4>(a, (uint32_t)(local % tpc), (uint32_t)(local / tpc), smem);
-      } else if (kind == FK_BITREV) {
-        const uint32_t L = E.log_rows;
-        const uint64_t n = 1ull << L, chunks = (n + FUSED_THREADS - 1) / FUSED_THREADS;
-        const uint64_t col = local / chunks, i = (local % chunks) * FUSED_THREADS + tid;
-        if (i < n) {
-          const uint64_t r = brev_low((uint32_t)i, L);
-          if (i < r) {
-            uint64_t *x = E.dst + col * E.stride;
-            const uint64_t vi = x[i], vr = x[r];
-            x[i] = vr;
-            x[r] = vi;
-          }
+  while (true) {
+    __syncthreads();  // the previous item's last reads of s_unit and of shared memory are done
+    if (tid == 0) s_unit = atomicAdd(next_unit, 1ull);
+    __syncthreads();
+    const uint64_t u = s_unit;
+    if (u >= total_units) break;
+    // the entry holding item u: the last one whose first item is <= u (uniform per CTA)
+    uint32_t lo = 0, hi = n_entries - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (entries[mid].first <= u)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const FusedEntry &E = entries[lo];
+    if (tid == 0 && E.dep != NO_COUNTER) {
+      // after one expired wait (a bug, not a slow producer) no item waits any more: the launch
+      // then ends within one wait limit whatever else is wrong
+      uint32_t it = 0;
+      while (ld_acquire(counters + E.dep) < E.dep_target && !ld_acquire(abort_flag)) {
+        if (++it > FUSED_WAIT_LIMIT) {
+          atomicAdd(&g_fused_timeouts, 1ull);
+          atomicExch(abort_flag, 1u);
+          break;
         }
-      } else if (kind == FK_LEAVES) {
-        const uint64_t gid = local * FUSED_THREADS + tid;
-        if (gid < E.count) leaf_hash<2, true>(E.src, E.dst, 0, E.cols, E.count, false, false, gid);
-      } else if (kind == FK_NODES) {
-        const uint64_t i = local * FUSED_THREADS + tid, count = E.count;
-        if (i < count) {
-          uint64_t l[4], r[4], o[4];
-          load_children(E.src, count, i, l, r, E.aux != 0);
-          hash_node<2, true>(l, r, o);
-#pragma unroll
-          for (int k = 0; k < 4; k++) E.dst[k * count + i] = o[k];
-        }
-      } else {  // FK_CAPS: cap[j*ccap*f + c*ccap + m] = tree_c[cap_off + j*ccap + m]
-        const uint64_t t = local * FUSED_THREADS + tid;
-        if (t < E.count) {
-          const uint64_t ccap = E.ccap, f = E.cols;
-          const uint64_t m = t % ccap, c = (t / ccap) % f, j = t / (ccap * f);
-          E.dst[j * ccap * f + c * ccap + m] = E.src[c * E.stride + E.aux + j * ccap + m];
-        }
+        __nanosleep(200);
       }
     }
-    grid.sync();
+    __syncthreads();  // the acquire above orders the producers' writes before this CTA's reads
+    const uint64_t local = u - E.first;
+    const uint32_t kind = E.kind;
+    if (kind == FK_NTT) {
+      const PassArgs a = E.ntt;
+      const uint64_t tpc = E.tiles_per_col;
+      ntt_pass_tile<4>(a, (uint32_t)(local % tpc), (uint32_t)(local / tpc), smem);
+    } else if (kind == FK_BITREV) {
+      const uint32_t L = E.log_rows;
+      const uint64_t n = 1ull << L, chunks = (n + FUSED_THREADS - 1) / FUSED_THREADS;
+      const uint64_t col = local / chunks, i = (local % chunks) * FUSED_THREADS + tid;
+      if (i < n) {
+        const uint64_t r = brev_low((uint32_t)i, L);
+        if (i < r) {
+          uint64_t *x = E.dst + col * E.stride;
+          const uint64_t vi = x[i], vr = x[r];
+          x[i] = vr;
+          x[r] = vi;
+        }
+      }
+    } else if (kind == FK_LEAVES) {
+      const uint64_t gid = local * FUSED_THREADS + tid;
+      if (gid < E.count) leaf_hash<2, true>(E.src, E.dst, 0, E.cols, E.count, false, false, gid);
+    } else if (kind == FK_NODES) {
+      const uint64_t i = local * FUSED_THREADS + tid, count = E.count;
+      if (i < count) {
+        uint64_t l[4], r[4], o[4];
+        load_children(E.src, count, i, l, r, E.aux != 0);
+        hash_node<2, true>(l, r, o);
+#pragma unroll
+        for (int k = 0; k < 4; k++) E.dst[k * count + i] = o[k];
+      }
+    } else {  // FK_CAPS: cap[j*ccap*f + c*ccap + m] = tree_c[cap_off + j*ccap + m]
+      const uint64_t t = local * FUSED_THREADS + tid;
+      if (t < E.count) {
+        const uint64_t ccap = E.ccap, f = E.cols;
+        const uint64_t m = t % ccap, c = (t / ccap) % f, j = t / (ccap * f);
+        E.dst[j * ccap * f + c * ccap + m] = E.src[c * E.stride + E.aux + j * ccap + m];
+      }
+    }
+    __syncthreads();  // every thread's writes of this item precede the release below
+    if (tid == 0) {
+      if (E.done1 != NO_COUNTER) red_release_add(counters + E.done1, 1u);
+      if (E.done2 != NO_COUNTER) red_release_add(counters + E.done2, 1u);
+    }
   }
 }
 
-// Host side: builds the step table of a batch and launches the persistent grid.
+// Host side: the work list of a batch (stages in order, items numbered globally, each entry
+// with its dependency counter) and the launch of the persistent grid.
 struct FusedPlan {
   std::vector<FusedEntry> entries;
-  std::vector<FusedStep> steps;
+  std::vector<uint32_t> target;  // per counter: the items that count into it
+  std::vector<std::vector<FusedEntry>> stages;
   size_t smem = 0;
 
-  void begin_step() { steps.push_back({(uint32_t)entries.size(), 0, 0}); }
-  void add(FusedEntry e) {
-    FusedStep &s = steps.back();
-    e.first = s.units;
-    s.units += e.units;
-    s.entries++;
-    entries.push_back(e);
+  uint32_t counter() {
+    target.push_back(0);
+    return (uint32_t)target.size() - 1;
   }
-  void end_step() {
-    if (steps.back().entries == 0) steps.pop_back();
+  void begin_stage() { stages.emplace_back(); }
+  void add(FusedEntry e, uint32_t dep, uint32_t done1, uint32_t done2 = NO_COUNTER) {
+    e.dep = dep;
+    e.done1 = done1;
+    e.done2 = done2;
+    if (done1 != NO_COUNTER) target[done1] += (uint32_t)e.units;
+    if (done2 != NO_COUNTER) target[done2] += (uint32_t)e.units;
+    if (e.units) stages.back().push_back(e);
+  }
+  // Heaviest items of each stage first (the last items to start bound a stage's tail), then the
+  // global numbering and the wait targets.
+  uint64_t finish() {
+    uint64_t first = 0;
+    for (auto &st : stages) {
+      std::stable_sort(st.begin(), st.end(), [](const FusedEntry &x, const FusedEntry &y) { return cost(x) > cost(y); });
+      for (FusedEntry &e : st) {
+        e.first = first;
+        first += e.units;
+        e.dep_target = e.dep == NO_COUNTER ? 0 : target[e.dep];
+        entries.push_back(e);
+      }
+    }
+    return first;
+  }
+  static uint64_t cost(const FusedEntry &e) {
+    if (e.kind == FK_NTT) return (1ull << (e.ntt.k + e.ntt.log_w)) * e.ntt.k * e.ntt.cols_per_cta;
+    if (e.kind == FK_LEAVES) return 4096 * ((e.cols + 7) / 8);
+    return 1;
   }
 };
 
@@ -157,15 +222,17 @@ static FusedEntry ntt_entry(const DeviceTables *t, uint32_t log_n, uint32_t q, u
   return e;
 }
 
-static int fused_plan(const DeviceTables *t, const glc_commit_job *jobs, uint32_t n_jobs, FusedPlan &P) {
+static uint64_t fused_plan(const DeviceTables *t, const glc_commit_job *jobs, uint32_t n_jobs, FusedPlan &P) {
   auto units = [](uint64_t n) { return (n + FUSED_THREADS - 1) / FUSED_THREADS; };
   struct J {
     const glc_commit_job *j;
     uint64_t n, f, coset_elems;
     uint64_t *mono;
     Pass inv[2], fwd[2];
-    uint32_t np;
-    uint32_t layers;  // tree layers including the leaves
+    uint32_t np, layers;  // NTT passes; tree layers including the leaves
+    bool in_place_last;   // the last coset transforms the monomials in place
+    uint32_t c_inv[2], c_brev, c_readers, c_trees;
+    std::vector<uint32_t> c_fwd0, c_fwd1, c_layer;  // per coset (c_layer: the latest layer built)
   };
   std::vector<J> js(n_jobs);
   uint32_t max_layers = 0;
@@ -175,29 +242,42 @@ static int fused_plan(const DeviceTables *t, const glc_commit_job *jobs, uint32_
     x.n = 1ull << jobs[i].log_n;
     x.f = 1ull << jobs[i].log_lde;
     x.coset_elems = x.n * jobs[i].cols;
+    x.in_place_last = !jobs[i].monomials;
     x.mono = jobs[i].monomials ? jobs[i].monomials : jobs[i].lde + (x.f - 1) * x.coset_elems;
     const NttTuning &tu = ntt_tuning(jobs[i].log_n);
     x.np = make_plan(jobs[i].log_n, false, tu, x.inv);
     make_plan(jobs[i].log_n, false, tu, x.fwd);
-    // tiles of at most 2^12 elements: 96 KB of shared memory at most, two CTAs per SM
+    // tiles of at most 2^12 elements: at most 64 KB of shared memory, three CTAs per SM
     for (uint32_t q = 0; q < x.np; q++) {
       x.inv[q].log_w = std::min(x.inv[q].log_w, SINGLE_PASS_MAX_LOG - x.inv[q].k);
       x.fwd[q].log_w = std::min(x.fwd[q].log_w, SINGLE_PASS_MAX_LOG - x.fwd[q].k);
     }
     x.layers = jobs[i].log_n - (jobs[i].log_cap - jobs[i].log_lde) + 1;
     max_layers = std::max(max_layers, x.layers);
+    x.c_inv[0] = P.counter();
+    x.c_inv[1] = P.counter();
+    x.c_brev = P.counter();
+    x.c_readers = P.counter();
+    x.c_trees = P.counter();
+    x.c_fwd0.resize(x.f);
+    x.c_fwd1.resize(x.f);
+    x.c_layer.resize(x.f);
+    for (uint64_t c = 0; c < x.f; c++) {
+      x.c_fwd0[c] = P.counter();
+      x.c_fwd1[c] = P.counter();
+    }
   }
   // inverse NTT (evaluations -> bit-reversed coefficients x N^-1), pass by pass
   for (uint32_t q = 0; q < 2; q++) {
-    P.begin_step();
+    P.begin_stage();
     for (J &x : js)
       if (q < x.np)
         P.add(ntt_entry(t, x.j->log_n, q, x.np, x.inv[q], x.j->evals, x.mono, x.j->evals_stride, x.n, x.j->cols, true, 0,
-                        0, P.smem));
-    P.end_step();
+                        0, P.smem),
+              q ? x.c_inv[0] : NO_COUNTER, x.c_inv[q]);
   }
   // bit reversal: natural-order monomials
-  P.begin_step();
+  P.begin_stage();
   for (J &x : js) {
     FusedEntry e{};
     e.kind = FK_BITREV;
@@ -205,27 +285,33 @@ static int fused_plan(const DeviceTables *t, const glc_commit_job *jobs, uint32_
     e.dst = x.mono;
     e.stride = x.n;
     e.units = (uint64_t)x.j->cols * units(x.n);
-    P.add(e);
+    P.add(e, x.c_inv[x.np - 1], x.c_brev);
   }
-  P.end_step();
   // forward coset NTTs; without a monomials buffer the last coset transforms the monomials in
-  // place, so it runs after the steps of the other cosets, which read them
+  // place, so its first pass waits until the other cosets' first passes have read them
   for (int last = 0; last < 2; last++)
     for (uint32_t q = 0; q < 2; q++) {
-      P.begin_step();
+      P.begin_stage();
       for (J &x : js) {
         if (q >= x.np) continue;
         for (uint64_t c = 0; c < x.f; c++) {
-          const bool in_place_last = !x.j->monomials && c == x.f - 1;
-          if (in_place_last != (last == 1)) continue;
-          P.add(ntt_entry(t, x.j->log_n, q, x.np, x.fwd[q], x.mono, x.j->lde + c * x.coset_elems, x.n, x.n, x.j->cols,
-                          false, x.j->log_lde, fused_brev((uint32_t)c, x.j->log_lde), P.smem));
+          const bool ipl = x.in_place_last && c == x.f - 1;
+          if (ipl != (last == 1)) continue;
+          const FusedEntry e = ntt_entry(t, x.j->log_n, q, x.np, x.fwd[q], x.mono, x.j->lde + c * x.coset_elems, x.n,
+                                         x.n, x.j->cols, false, x.j->log_lde, fused_brev((uint32_t)c, x.j->log_lde),
+                                         P.smem);
+          const uint32_t done = q ? x.c_fwd1[c] : x.c_fwd0[c];
+          if (q == 1)
+            P.add(e, x.c_fwd0[c], done);
+          else if (!ipl)
+            P.add(e, x.c_brev, done, x.in_place_last ? x.c_readers : NO_COUNTER);
+          else
+            P.add(e, x.f > 1 ? x.c_readers : x.c_brev, done);
         }
       }
-      P.end_step();
     }
   // leaf hashes of every coset
-  P.begin_step();
+  P.begin_stage();
   for (J &x : js)
     for (uint64_t c = 0; c < x.f; c++) {
       FusedEntry e{};
@@ -235,12 +321,12 @@ static int fused_plan(const DeviceTables *t, const glc_commit_job *jobs, uint32_
       e.count = x.n;
       e.cols = x.j->cols;
       e.units = units(x.n);
-      P.add(e);
+      x.c_layer[c] = P.counter();
+      P.add(e, x.np == 2 ? x.c_fwd1[c] : x.c_fwd0[c], x.c_layer[c], x.layers == 1 ? x.c_trees : NO_COUNTER);
     }
-  P.end_step();
   // node layers: layer l (parent count n >> l) starts at 8n - 8n / 2^l in the subtree buffer
   for (uint32_t l = 1; l < max_layers; l++) {
-    P.begin_step();
+    P.begin_stage();
     for (J &x : js) {
       if (l >= x.layers) continue;
       for (uint64_t c = 0; c < x.f; c++) {
@@ -252,13 +338,14 @@ static int fused_plan(const DeviceTables *t, const glc_commit_job *jobs, uint32_
         e.count = x.n >> l;
         e.aux = (reinterpret_cast<uintptr_t>(e.src) & 15) == 0;
         e.units = units(e.count);
-        P.add(e);
+        const uint32_t prev = x.c_layer[c];
+        x.c_layer[c] = P.counter();
+        P.add(e, prev, x.c_layer[c], l + 1 == x.layers ? x.c_trees : NO_COUNTER);
       }
     }
-    P.end_step();
   }
-  // caps
-  P.begin_step();
+  // caps, once every subtree of the job is built
+  P.begin_stage();
   for (J &x : js) {
     const uint32_t ccap = 1u << (x.j->log_cap - x.j->log_lde);
     FusedEntry e{};
@@ -271,10 +358,9 @@ static int fused_plan(const DeviceTables *t, const glc_commit_job *jobs, uint32_
     e.cols = x.f;
     e.count = 4ull * ccap * x.f;
     e.units = units(e.count);
-    P.add(e);
+    P.add(e, x.c_trees, NO_COUNTER);
   }
-  P.end_step();
-  return 0;
+  return P.finish();
 }
 
 }  // namespace glc
@@ -292,8 +378,8 @@ extern "C" glc_status glc_commit_batch_fused(const glc_commit_job *jobs, uint32_
   const DeviceTables *t = current_tables();
   if (!t) return fail("commit_batch_fused: glc_context_create has not been called on this device");
   FusedPlan P;
-  int e = fused_plan(t, jobs, n_jobs, P);
-  if (e) return e;
+  const uint64_t total = fused_plan(t, jobs, n_jobs, P);
+  if (P.entries.empty()) return 0;
   cudaStream_t stream = (cudaStream_t)stream_;
   cudaError_t ce = cudaFuncSetAttribute(fused_commit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem);
   int dev = 0, sms = 0, per_sm = 0;
@@ -303,22 +389,35 @@ extern "C" glc_status glc_commit_batch_fused(const glc_commit_job *jobs, uint32_
     ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_commit_kernel, FUSED_THREADS, P.smem);
   if (ce != cudaSuccess) return (int)ce;
   if (per_sm < 1) return fail("commit_batch_fused: the kernel does not fit on an SM");
-  const size_t eb = P.entries.size() * sizeof(FusedEntry), sb = P.steps.size() * sizeof(FusedStep);
+  // one stream-ordered buffer: the entries, then the counters and the item counter (zeroed)
+  const size_t eb = P.entries.size() * sizeof(FusedEntry);
+  const size_t cb = ((P.target.size() + 1) * sizeof(uint32_t) + 7) / 8 * 8 + sizeof(unsigned long long);
   char *buf = nullptr;
-  ce = cudaMallocAsync((void **)&buf, eb + sb, stream);
+  ce = cudaMallocAsync((void **)&buf, eb + cb, stream);
   if (ce != cudaSuccess) return (int)ce;
-  // pageable source: the copies are staged before they return, so the host tables may go
+  // pageable source: the copy is staged before it returns, so the host table may go
   ce = cudaMemcpyAsync(buf, P.entries.data(), eb, cudaMemcpyHostToDevice, stream);
-  if (ce == cudaSuccess) ce = cudaMemcpyAsync(buf + eb, P.steps.data(), sb, cudaMemcpyHostToDevice, stream);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(buf + eb, 0, cb, stream);
   if (ce == cudaSuccess) {
     const FusedEntry *de = reinterpret_cast<const FusedEntry *>(buf);
-    const FusedStep *ds = reinterpret_cast<const FusedStep *>(buf + eb);
-    uint32_t ns = (uint32_t)P.steps.size();
-    void *args[] = {(void *)&de, (void *)&ds, (void *)&ns};
+    uint32_t *counters = reinterpret_cast<uint32_t *>(buf + eb);
+    uint32_t *abort_flag = counters + P.target.size();
+    unsigned long long *next = reinterpret_cast<unsigned long long *>(buf + eb + cb - sizeof(unsigned long long));
+    uint32_t ne = (uint32_t)P.entries.size();
+    uint64_t tu = total;
+    void *args[] = {(void *)&de, (void *)&ne, (void *)&tu, (void *)&counters, (void *)&abort_flag, (void *)&next};
     ce = cudaLaunchCooperativeKernel((const void *)fused_commit_kernel, dim3((unsigned)(per_sm * sms)),
                                      dim3(FUSED_THREADS), args, P.smem, stream);
     count_launches(1);
   }
   const cudaError_t fe = cudaFreeAsync(buf, stream);
   return (int)(ce != cudaSuccess ? ce : fe);
+}
+
+extern "C" glc_status glc_commit_batch_fused_timeouts(uint64_t *out) {
+  if (!out) return fail("commit_batch_fused_timeouts: null output");
+  unsigned long long v = 0;
+  const cudaError_t e = cudaMemcpyFromSymbol(&v, g_fused_timeouts, sizeof(v));
+  *out = v;
+  return (int)e;
 }
