@@ -30,26 +30,22 @@ __device__ __forceinline__ uint64_t madw(uint32_t a, uint32_t b, uint64_t c) {
 
 // a + b mod p, inputs and output in [0, 2^64).  A carry out of 64 bits is worth EPS; adding it
 // through a second carry chain wraps again only when the first wrapped sum is >= p, and that
-// second carry (EPS once more) cannot wrap: the first wrapped sum is at most 2^64 - 2.  Both
-// corrections stay on the ALU pipe (the carry, negated, is EPS's low word; its high word is 0).
+// second carry (EPS once more) cannot wrap: the first wrapped sum is at most 2^64 - 2.
 __device__ __forceinline__ uint64_t add(uint64_t a, uint64_t b) {
-  uint32_t r0, r1;
+  uint32_t r0, r1, c2;
   asm("{\n\t"
       ".reg .u32 c;\n\t"
-      "add.cc.u32 %0, %2, %4;\n\t"
-      "addc.cc.u32 %1, %3, %5;\n\t"
+      "add.cc.u32 %0, %3, %5;\n\t"
+      "addc.cc.u32 %1, %4, %6;\n\t"
       "addc.u32 c, 0, 0;\n\t"
-      "neg.s32 c, c;\n\t"
+      "neg.s32 c, c;\n\t"           // 0 or 0xFFFFFFFF = EPS's low word
       "add.cc.u32 %0, %0, c;\n\t"
       "addc.cc.u32 %1, %1, 0;\n\t"
-      "addc.u32 c, 0, 0;\n\t"
-      "neg.s32 c, c;\n\t"
-      "add.cc.u32 %0, %0, c;\n\t"
-      "addc.u32 %1, %1, 0;\n\t"
+      "addc.u32 %2, 0, 0;\n\t"
       "}"
-      : "=r"(r0), "=r"(r1)
+      : "=r"(r0), "=r"(r1), "=r"(c2)
       : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
-  return pack(r0, r1);
+  return madw(c2, 0xFFFFFFFFu, pack(r0, r1));
 }
 
 // a - b mod p.  A borrow is worth -EPS; subtracting it borrows again only when the wrapped

@@ -57,13 +57,6 @@ __device__ __forceinline__ uint64_t coset_power(const PassArgs &a, uint32_t j) {
   return f;
 }
 
-// Slot of block twiddle m of a level u rounds into the last radix round: the low u bits are XORed
-// with bits 4..4+u-1 (a permutation of the level's slots, u <= 3).  In that round the threads of
-// a contiguous tile (log_w = 0) read twiddles m = q * 2^u + c; unswizzled, 32 threads spread
-// over 2^u times the two 128-byte wavefronts they need, and the XOR spreads them back over 16
-// distinct 8-byte slots of one 256-byte window.
-__device__ __forceinline__ uint32_t tw_slot(uint32_t m, uint32_t u) { return m ^ ((m >> 4) & ((1u << u) - 1)); }
-
 __device__ __forceinline__ uint32_t brev_low(uint32_t x, uint32_t bits) { return bits ? __brev(x) >> (32 - bits) : 0; }
 
 template <uint32_t R, bool DIF>
@@ -87,7 +80,7 @@ __device__ __forceinline__ void radix_round(uint64_t *tile, const uint64_t *tws,
       for (uint32_t j = 0; j < (1u << R); j++) {
         if (j & (1u << bit)) continue;
         const uint32_t m = mb | (j >> (R - u));
-        const uint64_t w = tws[(1u << level) - 1 + (k == t + R ? tw_slot(m, u) : m)];
+        const uint64_t w = tws[(1u << level) - 1 + m];
         const uint64_t x = v[j], y = v[j | (1u << bit)];
         if (!DIF) {
           const uint64_t yw = mul(y, w);
@@ -140,12 +133,11 @@ __device__ __forceinline__ void ntt_pass_tile(const PassArgs &a, uint32_t bx, ui
     if (threadIdx.x < k) sig[threadIdx.x] = coset_power(a, 1u << (a.log_n - 1 - a.s0 - threadIdx.x));
     __syncthreads();
   }
-  const uint32_t t_last = ((k - 1) / RB) * RB;  // first level of the last radix round
   for (uint32_t idx = threadIdx.x; idx + 1 < (1u << k); idx += blockDim.x) {
     const uint32_t t = 31 - __clz(idx + 1);
     const uint32_t m = idx + 1 - (1u << t);
     const uint64_t w = a.tw[((uint64_t)hi << t) + m];
-    tws[(1u << t) - 1 + (t >= t_last ? tw_slot(m, t - t_last) : m)] = a.fold ? mul(w, sig[t]) : w;
+    tws[idx] = a.fold ? mul(w, sig[t]) : w;
   }
   // Coset / size scaling as two per-CTA tables: the exponent j of element (mid, w) splits as
   //   natural j = mid * M + (lo0 + w)                      (strided pass, hi = 0)
