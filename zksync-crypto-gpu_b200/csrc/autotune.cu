@@ -113,7 +113,7 @@ extern "C" glc_status glc_autotune(uint32_t log_n_min, uint32_t log_n_max, uint3
         if (k + 3 >= log_n / 2 && k <= log_n / 2 + 3) k1s.push_back(k);
     for (uint32_t rb : {2u, 3u, 4u})
       for (uint32_t k1 : k1s)
-        for (uint32_t lw : {3u, 4u, 5u})
+        for (uint32_t lw : {2u, 3u, 4u, 5u})
           for (uint32_t cpc : {1u, 4u, 8u})
             for (uint32_t mb : {0u, 48u}) {
             if (err || (mb && log_n <= 12)) continue;  // stop after an error; one pass: nothing to chunk

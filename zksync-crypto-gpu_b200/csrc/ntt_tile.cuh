@@ -18,7 +18,7 @@ static constexpr uint32_t PASS_THREADS = 512;
 __host__ __device__ constexpr uint32_t pass_threads(uint32_t rb) { return rb >= 4 ? 256 : PASS_THREADS; }
 __host__ __device__ constexpr uint32_t pass_min_blocks(uint32_t rb) { return rb >= 4 ? 3 : 2; }
 static constexpr uint32_t SINGLE_PASS_MAX_LOG = 12;
-static constexpr int NTT_SMEM_MAX = 140 * 1024;  // tile 64 KiB + twiddles 32 KiB + scaling tables 32 KiB  // one column per tile, tile + twiddles <= 64 KiB
+static constexpr int NTT_SMEM_MAX = 140 * 1024;  // tile 68 KiB + twiddles 34 KiB + scaling tables 32 KiB (padded)
 
 struct PassArgs {
   const uint64_t *in;
@@ -40,7 +40,16 @@ struct PassArgs {
   const uint64_t *w_lo, *w_hi;  // powers of w_{2^30}
 };
 
-__device__ __forceinline__ uint32_t swz(uint32_t e) { return e ^ ((e >> 4) & 15u); }
+// Shared-memory slot of tile element e: one padding slot after every 16 elements.  Every radix
+// round's accesses are free of bank conflicts in this layout (a warp's 32 8-byte accesses cover 16
+// distinct bank pairs twice), and the map is additive on the index sets a round touches: for a
+// round base b whose bits p .. p+R-1 are zero, pad(b | j << p) = pad(b) + pad(j << p), and
+// pad(j << p) = j * pad(1 << p) when p >= 4.  A thread's 2^R slots are thus one base slot plus
+// per-round offsets (multiples of one stride when p >= 4).
+__host__ __device__ constexpr uint32_t pad(uint32_t e) { return e + (e >> 4); }
+// Block twiddle idx (heap order: level l holds idx 2^l - 1 .. 2^(l+1) - 2) sits in slot
+// pad(idx + 1) - 1: each level padded like the tile, so a thread's twiddles of one level are one
+// base slot plus its small index.
 
 // s^j (scale 1) or s^-j (scale 2) for the coset shift s = g * w_{2^(L+e)}^c; 1 without extension
 __device__ __forceinline__ uint64_t coset_power(const PassArgs &a, uint32_t j) {
@@ -59,28 +68,30 @@ __device__ __forceinline__ uint64_t coset_power(const PassArgs &a, uint32_t j) {
 
 __device__ __forceinline__ uint32_t brev_low(uint32_t x, uint32_t bits) { return bits ? __brev(x) >> (32 - bits) : 0; }
 
-template <uint32_t R, bool DIF>
+template <uint32_t R, bool DIF, bool LIN>
 __device__ __forceinline__ void radix_round(uint64_t *tile, const uint64_t *tws, uint32_t k, uint32_t log_w, uint32_t t) {
   const uint32_t log_e = k + log_w;
   const uint32_t p = k - t - R + log_w;  // lowest active bit of the tile index
   const uint32_t jobs = 1u << (log_e - R);
+  const uint32_t S = pad(1u << p);       // slot stride of the round's elements when LIN (p >= 4)
   for (uint32_t q = threadIdx.x; q < jobs; q += blockDim.x) {
     const uint32_t base = ((q >> p) << (p + R)) | (q & ((1u << p) - 1));
     const uint32_t mid_base = base >> log_w;
+    uint64_t *tb = tile + pad(base);
     uint64_t v[1 << R];
 #pragma unroll
-    for (uint32_t j = 0; j < (1u << R); j++) v[j] = tile[swz(base | (j << p))];
+    for (uint32_t j = 0; j < (1u << R); j++) v[j] = tb[LIN ? j * S : pad(j << p)];
 #pragma unroll
     for (uint32_t uu = 0; uu < R; uu++) {
       const uint32_t u = DIF ? R - 1 - uu : uu;
       const uint32_t level = t + u;
       const uint32_t bit = R - 1 - u;
-      const uint32_t mb = mid_base >> (k - level);
+      // twiddle m = mb + jj (jj < 2^u, mb with zero low u bits): slot pad(2^level + mb) - 1 + jj
+      const uint64_t *tl = tws + pad((1u << level) + (mid_base >> (k - level))) - 1;
 #pragma unroll
       for (uint32_t j = 0; j < (1u << R); j++) {
         if (j & (1u << bit)) continue;
-        const uint32_t m = mb | (j >> (R - u));
-        const uint64_t w = tws[(1u << level) - 1 + m];
+        const uint64_t w = tl[j >> (R - u)];
         const uint64_t x = v[j], y = v[j | (1u << bit)];
         if (!DIF) {
           const uint64_t yw = mul(y, w);
@@ -93,21 +104,29 @@ __device__ __forceinline__ void radix_round(uint64_t *tile, const uint64_t *tws,
       }
     }
 #pragma unroll
-    for (uint32_t j = 0; j < (1u << R); j++) tile[swz(base | (j << p))] = v[j];
+    for (uint32_t j = 0; j < (1u << R); j++) tb[LIN ? j * S : pad(j << p)] = v[j];
   }
+}
+
+template <uint32_t R, bool DIF>
+__device__ __forceinline__ void radix_round_p(uint64_t *tile, const uint64_t *tws, uint32_t k, uint32_t log_w, uint32_t t) {
+  if (k + log_w >= t + R + 4)  // p >= 4: slots of the round's elements are multiples of one stride
+    radix_round<R, DIF, true>(tile, tws, k, log_w, t);
+  else
+    radix_round<R, DIF, false>(tile, tws, k, log_w, t);
 }
 
 template <bool DIF, uint32_t RB>
 __device__ __forceinline__ void round_dispatch(uint64_t *tile, const uint64_t *tws, uint32_t k, uint32_t log_w, uint32_t t,
                                                uint32_t r) {
   if (RB >= 4 && r == 4)
-    radix_round<(RB >= 4 ? 4 : 1), DIF>(tile, tws, k, log_w, t);
+    radix_round_p<(RB >= 4 ? 4 : 1), DIF>(tile, tws, k, log_w, t);
   else if (RB >= 3 && r == 3)
-    radix_round<(RB >= 3 ? 3 : 1), DIF>(tile, tws, k, log_w, t);
+    radix_round_p<(RB >= 3 ? 3 : 1), DIF>(tile, tws, k, log_w, t);
   else if (r == 2)
-    radix_round<2, DIF>(tile, tws, k, log_w, t);
+    radix_round<2, DIF, false>(tile, tws, k, log_w, t);
   else
-    radix_round<1, DIF>(tile, tws, k, log_w, t);
+    radix_round<1, DIF, false>(tile, tws, k, log_w, t);
 }
 
 // One CTA's share of a pass: tile bx of column group by (what the ntt_pass_kernel CTA with block
@@ -118,13 +137,13 @@ __device__ __forceinline__ void ntt_pass_tile(const PassArgs &a, uint32_t bx, ui
   const uint32_t k = a.k, log_w = a.log_w;
   const uint32_t E = 1u << (k + log_w);
   uint64_t *tile = smem;
-  uint64_t *tws = smem + E;
+  uint64_t *tws = smem + pad(E);
   const uint32_t log_m = a.log_n - a.s0 - k;
   const uint32_t log_tph = log_m - log_w;
   const uint32_t hi = bx >> log_tph;
   const uint32_t lo0 = (bx & ((1u << log_tph) - 1)) << log_w;
   const uint64_t base_i = ((uint64_t)hi << (a.log_n - a.s0)) + lo0;
-  // tws[2^t - 1 + m] = T[hi * 2^t + m]: block twiddles of stage s0 + t for this hi.
+  // block twiddle 2^t - 1 + m = T[hi * 2^t + m]: twiddles of stage s0 + t for this hi.
   // Folded coset NTT: DFT(x_j s^j) splits at every stage into two half-size problems whose
   // cosets differ by the stage's twiddle, so each block twiddle of stage u gains the factor
   // s^(2^(L-1-u)) and the x s^j scaling disappears from the data path.
@@ -137,13 +156,13 @@ __device__ __forceinline__ void ntt_pass_tile(const PassArgs &a, uint32_t bx, ui
     const uint32_t t = 31 - __clz(idx + 1);
     const uint32_t m = idx + 1 - (1u << t);
     const uint64_t w = a.tw[((uint64_t)hi << t) + m];
-    tws[idx] = a.fold ? mul(w, sig[t]) : w;
+    tws[pad(idx + 1) - 1] = a.fold ? mul(w, sig[t]) : w;
   }
   // Coset / size scaling as two per-CTA tables: the exponent j of element (mid, w) splits as
   //   natural j = mid * M + (lo0 + w)                      (strided pass, hi = 0)
   //   bit-reversed j = bitrev_k(mid) << (L - k) + bitrev_{L-k}(hi)  (contiguous pass, W = 1)
   // so the factor is P[mid] * Q[w] (P carries N^-1 on the inverse side): 2 multiplies per element.
-  uint64_t *Pt = tws + (1u << k);
+  uint64_t *Pt = tws + pad(1u << k);
   uint64_t *Qt = Pt + (1u << k);
   if (a.scale == 1 || (a.scale == 2 && a.log_ext)) {
     for (uint32_t m = threadIdx.x; m < (1u << k); m += blockDim.x) {
@@ -169,15 +188,15 @@ __device__ __forceinline__ void ntt_pass_tile(const PassArgs &a, uint32_t bx, ui
       for (uint32_t e = 2 * threadIdx.x; e < E; e += 2 * blockDim.x) {
         const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
         const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(src + i);
-        tile[swz(e)] = v.x;
-        tile[swz(e + 1)] = v.y;
+        tile[pad(e)] = v.x;
+        tile[pad(e + 1)] = v.y;
       }
     } else {
       for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
         const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
         uint64_t v = src[i];
         if (a.scale == 1) v = mul(v, mul(Pt[e >> log_w], Qt[a.j_bitrev ? 0u : (e & wmask)]));
-        tile[swz(e)] = v;
+        tile[pad(e)] = v;
       }
     }
     __syncthreads();
@@ -197,7 +216,7 @@ __device__ __forceinline__ void ntt_pass_tile(const PassArgs &a, uint32_t bx, ui
     if (a.vec2) {
       for (uint32_t e = 2 * threadIdx.x; e < E; e += 2 * blockDim.x) {
         const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
-        uint64_t v0 = tile[swz(e)], v1 = tile[swz(e + 1)];
+        uint64_t v0 = tile[pad(e)], v1 = tile[pad(e + 1)];
         if (a.scale == 2) {
           v0 = mul(v0, a.n_inv);
           v1 = mul(v1, a.n_inv);
@@ -211,7 +230,7 @@ __device__ __forceinline__ void ntt_pass_tile(const PassArgs &a, uint32_t bx, ui
     } else {
       for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
         const uint64_t i = base_i + ((uint64_t)(e >> log_w) << log_m) + (e & wmask);
-        uint64_t v = tile[swz(e)];
+        uint64_t v = tile[pad(e)];
         if (a.scale == 2)
           v = a.log_ext ? mul(v, mul(Pt[e >> log_w], Qt[a.j_bitrev ? 0u : (e & wmask)])) : mul(v, a.n_inv);
         dst[i] = a.last ? canon(v) : v;  // a following pass accepts any value below 2^64
@@ -323,7 +342,7 @@ static inline PassShape make_pass(PassArgs &a, const DeviceTables *t, const NttT
   // pass without a coset multiplies by N^-1 only: no tables, and the 2^k-entry table it does not
   // need would cost a third CTA per SM on 2^12-element tiles)
   const bool tables = a.scale == 1 || (a.scale == 2 && a.log_ext);
-  sh.smem = ((size_t(1) << tile_log) + (size_t(1) << ps.k) +
+  sh.smem = ((size_t)pad(1u << tile_log) + pad(1u << ps.k) +
              (tables ? (size_t(1) << ps.k) + (size_t(1) << ps.log_w) : 0)) * sizeof(uint64_t);
   sh.threads = (uint32_t)std::min<uint64_t>(pass_threads(tu.radix_bits),
                                             std::max<uint64_t>(32, (1ull << tile_log) >> tu.radix_bits));
