@@ -11,16 +11,20 @@
 //   inverse NTT pass 1, pass 2 -> bit reversal -> forward coset NTT pass 1, pass 2 (the coset
 //   that transforms the monomials in place last, after the others have read them) -> leaf
 //   hashes -> node layer 1, 2, ... -> cap gather,
-// every stage listing the items of all jobs, heaviest first.  An item is an NTT tile, 256 rows of
-// a bit reversal, 256 leaves, 256 nodes or 256 cap entries.  Before it runs, an item waits until
-// the items it reads from are done: each stage of each job (per coset where it applies) counts
-// its finished items, and the item waits for its producer's count to reach the producer's item
-// total.  Items wait only for items that come earlier in the order, which some resident CTA
+// every stage listing the items of all jobs, heaviest first.  An item is an NTT tile of 2^12
+// elements (or a whole column of a smaller NTT) in up to two columns, 4096 rows of a bit reversal,
+// 256 leaves, 256 nodes or 256 cap entries: large enough that the per-item costs (the claim of
+// the item number, the search for its entry, the dependency check and the release of its count,
+// a few microseconds together) stay a few percent of its work.  Before it runs, an item waits
+// until the items it reads from are done: each stage of each job (per coset where it applies)
+// counts its finished items, and the item waits for its producer's count to reach the producer's
+// item total.  Items wait only for items that come earlier in the order, which some resident CTA
 // fetched already, so the grid always makes progress; different jobs' stages overlap freely.
 // Every wait is bounded (about 1 s): on expiry the item counts a timeout in a device counter
 // (glc_commit_batch_fused_timeouts), raises the launch's abort flag, which ends every other
-// wait, and runs anyway, so a bug shows as wrong results and a non-zero count, never as a hang.  The items reuse the tile and hash code of the per-call
-// kernels (ntt_pass_tile, leaf_hash, hash_node), so the results are the same bits.
+// wait, and runs anyway, so a bug shows as wrong results and a non-zero count, never as a hang.
+// The items reuse the tile and hash code of the per-call kernels (ntt_pass_tile, leaf_hash,
+// hash_node), so the results are the same bits.
 //
 // Included at the end of poseidon2.cu: it needs that file's __constant__ round constants.
 #pragma once
@@ -36,6 +40,10 @@ namespace cg = cooperative_groups;
 
 static constexpr uint32_t FUSED_THREADS = 256;
 static constexpr uint32_t FUSED_MAX_LOG_N = 16;
+// columns per NTT item (fewer when a job has fewer)
+static constexpr uint32_t FUSED_NTT_COLS = 2;
+// rows of one column per bit-reversal item
+static constexpr uint32_t FUSED_BITREV_ROWS = 4096;
 
 enum FusedKind : uint32_t { FK_NTT = 0, FK_BITREV = 1, FK_LEAVES = 2, FK_NODES = 3, FK_CAPS = 4 };
 
@@ -80,23 +88,40 @@ __global__ void __launch_bounds__(FUSED_THREADS, 3)
                         uint32_t *abort_flag, unsigned long long *next_unit) {
   extern __shared__ uint64_t smem[];
   __shared__ uint64_t s_unit;
+  __shared__ uint32_t s_entry;
   const uint32_t tid = threadIdx.x;
+  // Thread 0 claims the CTA's next item while the current one runs, so the claim's round trip
+  // to L2 is off the critical path.  Progress still holds: a CTA's claims increase, so the CTA
+  // that holds the lowest unfinished item is running it (its claimed-next item is above it),
+  // and that item's producers, all lower, are finished.
+  unsigned long long claimed = 0;
+  if (tid == 0) claimed = atomicAdd(next_unit, 1ull);
   while (true) {
-    __syncthreads();  // the previous item's last reads of s_unit and of shared memory are done
-    if (tid == 0) s_unit = atomicAdd(next_unit, 1ull);
+    __syncthreads();  // the previous item's last reads of s_unit, s_entry and shared memory are done
+    if (tid == 0) {
+      s_unit = claimed;
+      if (claimed < total_units) claimed = atomicAdd(next_unit, 1ull);
+    }
     __syncthreads();
     const uint64_t u = s_unit;
     if (u >= total_units) break;
-    // the entry holding item u: the last one whose first item is <= u (uniform per CTA)
-    uint32_t lo = 0, hi = n_entries - 1;
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi + 1) >> 1;
-      if (entries[mid].first <= u)
-        lo = mid;
-      else
-        hi = mid - 1;
+    // the entry holding item u, the last one whose first item is <= u: a 32-way search by warp 0
+    // (three rounds of dependent loads for up to 32K entries)
+    if (tid < 32) {
+      uint32_t lo = 0, span = n_entries;  // entries[lo].first <= u; the answer is below lo + span
+      while (span > 1) {
+        const uint32_t step = (span + 31) / 32;
+        const uint32_t idx = lo + tid * step;
+        const bool ok = idx < lo + span && entries[idx].first <= u;
+        const uint32_t last = 31 - __clz(__ballot_sync(0xFFFFFFFFu, ok));  // lane 0 is always ok
+        const uint32_t nlo = lo + last * step;
+        span = min(step, lo + span - nlo);
+        lo = nlo;
+      }
+      if (tid == 0) s_entry = lo;
     }
-    const FusedEntry &E = entries[lo];
+    __syncthreads();
+    const FusedEntry &E = entries[s_entry];
     if (tid == 0 && E.dep != NO_COUNTER) {
       // after one expired wait (a bug, not a slow producer) no item waits any more: the launch
       // then ends within one wait limit whatever else is wrong
@@ -119,12 +144,12 @@ __global__ void __launch_bounds__(FUSED_THREADS, 3)
       ntt_pass_tile<4>(a, (uint32_t)(local % tpc), (uint32_t)(local / tpc), smem);
     } else if (kind == FK_BITREV) {
       const uint32_t L = E.log_rows;
-      const uint64_t n = 1ull << L, chunks = (n + FUSED_THREADS - 1) / FUSED_THREADS;
-      const uint64_t col = local / chunks, i = (local % chunks) * FUSED_THREADS + tid;
-      if (i < n) {
+      const uint64_t n = 1ull << L, chunks = (n + FUSED_BITREV_ROWS - 1) / FUSED_BITREV_ROWS;
+      const uint64_t col = local / chunks, i0 = (local % chunks) * FUSED_BITREV_ROWS;
+      uint64_t *x = E.dst + col * E.stride;
+      for (uint64_t i = i0 + tid; i < min(i0 + FUSED_BITREV_ROWS, n); i += FUSED_THREADS) {
         const uint64_t r = brev_low((uint32_t)i, L);
         if (i < r) {
-          uint64_t *x = E.dst + col * E.stride;
           const uint64_t vi = x[i], vr = x[r];
           x[i] = vr;
           x[r] = vi;
@@ -207,6 +232,21 @@ static uint32_t fused_brev(uint32_t x, uint32_t bits) {
   return r;
 }
 
+// Passes of an NTT in the fused batch: tiles of 2^12 elements wherever the size allows, so the
+// items are few and large (each item rebuilds its tile's block twiddles and pays a claim, a
+// search and a dependency check): one pass up to 2^12 rows, else a strided pass of log_n - 12
+// stages over tiles of 2^(24 - log_n) columns and a contiguous pass of 12 stages.
+static uint32_t fused_ntt_plan(uint32_t log_n, Pass *p) {
+  if (log_n <= SINGLE_PASS_MAX_LOG) {
+    p[0] = {0, log_n, 0};
+    return 1;
+  }
+  const uint32_t k0 = log_n - SINGLE_PASS_MAX_LOG;
+  p[0] = {0, k0, SINGLE_PASS_MAX_LOG - k0};
+  p[1] = {k0, SINGLE_PASS_MAX_LOG, 0};
+  return 2;
+}
+
 static FusedEntry ntt_entry(const DeviceTables *t, uint32_t log_n, uint32_t q, uint32_t np, const Pass &ps,
                             const uint64_t *in, uint64_t *out, uint64_t in_stride, uint64_t out_stride, uint32_t cols,
                             bool inverse, uint32_t log_ext, uint32_t coset, size_t &smem) {
@@ -215,9 +255,11 @@ static FusedEntry ntt_entry(const DeviceTables *t, uint32_t log_n, uint32_t q, u
   NttTuning tu = ntt_tuning(log_n);
   tu.radix_bits = 4;
   const PassShape sh = make_pass(e.ntt, t, tu, ps, q, np, in, out, in_stride, out_stride, cols, log_n, false, inverse,
-                                 log_ext, coset, tu.max_cols_per_cta);
+                                 log_ext, coset, 1);
+  // the batch fills the device together: FUSED_NTT_COLS columns per item whatever the job's size
+  e.ntt.cols_per_cta = std::min(FUSED_NTT_COLS, cols);
   e.tiles_per_col = sh.tiles_per_col;
-  e.units = sh.tiles_per_col * sh.groups;
+  e.units = sh.tiles_per_col * ((cols + e.ntt.cols_per_cta - 1) / e.ntt.cols_per_cta);
   smem = std::max(smem, sh.smem);
   return e;
 }
@@ -244,14 +286,9 @@ static uint64_t fused_plan(const DeviceTables *t, const glc_commit_job *jobs, ui
     x.coset_elems = x.n * jobs[i].cols;
     x.in_place_last = !jobs[i].monomials;
     x.mono = jobs[i].monomials ? jobs[i].monomials : jobs[i].lde + (x.f - 1) * x.coset_elems;
-    const NttTuning &tu = ntt_tuning(jobs[i].log_n);
-    x.np = make_plan(jobs[i].log_n, false, tu, x.inv);
-    make_plan(jobs[i].log_n, false, tu, x.fwd);
-    // tiles of at most 2^12 elements: at most 64 KB of shared memory, three CTAs per SM
-    for (uint32_t q = 0; q < x.np; q++) {
-      x.inv[q].log_w = std::min(x.inv[q].log_w, SINGLE_PASS_MAX_LOG - x.inv[q].k);
-      x.fwd[q].log_w = std::min(x.fwd[q].log_w, SINGLE_PASS_MAX_LOG - x.fwd[q].k);
-    }
+    // tiles of at most 2^12 elements: at most 68 KB of shared memory, three CTAs per SM
+    x.np = fused_ntt_plan(jobs[i].log_n, x.inv);
+    fused_ntt_plan(jobs[i].log_n, x.fwd);
     x.layers = jobs[i].log_n - (jobs[i].log_cap - jobs[i].log_lde) + 1;
     max_layers = std::max(max_layers, x.layers);
     x.c_inv[0] = P.counter();
@@ -284,7 +321,7 @@ static uint64_t fused_plan(const DeviceTables *t, const glc_commit_job *jobs, ui
     e.log_rows = x.j->log_n;
     e.dst = x.mono;
     e.stride = x.n;
-    e.units = (uint64_t)x.j->cols * units(x.n);
+    e.units = (uint64_t)x.j->cols * ((x.n + FUSED_BITREV_ROWS - 1) / FUSED_BITREV_ROWS);
     P.add(e, x.c_inv[x.np - 1], x.c_brev);
   }
   // forward coset NTTs; without a monomials buffer the last coset transforms the monomials in
