@@ -137,5 +137,6 @@ extern "C" glc_status glc_context_destroy(void) {
   // cudaFree synchronises the device, so no kernel still reads the tables
   free_tables(g_tables[dev]);
   noalloc_forget_device(dev);
+  fused_forget_device(dev);
   return 0;
 }

@@ -86,6 +86,7 @@ int p2_tree_nodes_launch(uint64_t *layer0, uint64_t leaves, uint32_t layers, cud
 
 int ntt_init_device();  // kernel attributes; called by glc_context_create
 void noalloc_forget_device(int dev);  // drops the cached scratch address; called by glc_context_destroy
+void fused_forget_device(int dev);    // releases the fused batch's work-table pool; called by glc_context_destroy
 double job_cost(const glc_commit_job &j);
 int commit_check(const glc_commit_job &j);
 // Enqueues one job; when `events` is given, records events[0] before the first stage, one after
