@@ -852,6 +852,38 @@ def run_profile_case(args):
     ctx.destroy()
 
 
+def run_fused_trace(args):
+    """The fused launch on the uneven batch's small jobs (log2 rows <= 15), with its per-item
+    trace: where the CTAs spent their time (commit.fused_trace_summary) and the launch's time."""
+    glc, torch, ctx = _setup_device()
+    syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
+    jobs = [j for j in uneven_jobs() if j[0] <= 15]
+    bufs = []
+    for i, (l, c, e, cap) in enumerate(jobs):
+        sz = glc.CommitJob.sizes(l, c, e, cap)
+        dev = lambda k: torch.empty(sz[k], dtype=torch.int64, device="cuda")
+        bufs.append(glc.CommitJob(evals=dev("evals"), log_n=l, cols=c, log_lde=e, log_cap=cap, lde=dev("lde"),
+                                  trees=dev("trees"), cap=dev("cap")))
+        syn.fill_device(bufs[-1].evals, "uneven-0-%d" % i)
+    trace = torch.zeros(4 << 20, dtype=torch.int64, device="cuda")
+    for _ in range(max(args.warmup, 1)):
+        glc.commit.commit_batch_fused(bufs)
+    ms = []
+    for _ in range(max(args.steps, 1)):
+        trace.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        glc.commit.commit_batch_fused(bufs, trace=trace)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    summary = glc.commit.fused_trace_summary(trace.cpu().numpy().view("uint64"))
+    print(json.dumps({"workload": "fused launch, uneven batch small jobs (log2 rows <= 15): %d jobs" % len(jobs),
+                      "ms_per_launch": sorted(ms)[len(ms) // 2], "trace_of_last_launch": summary,
+                      "timeouts": glc.commit.fused_timeouts()}), flush=True)
+    ctx.destroy()
+
+
 def run_probe(args):
     """The modular-multiply probe alone (the roofline denominator), for instruction-mix captures."""
     glc, torch, ctx = _setup_device()
@@ -870,7 +902,7 @@ def main():
     ap.add_argument("--no-ref-kernels", action="store_true", help="skip the reference-kernel timing and parity leg")
     ap.add_argument("--no-extras", action="store_true", help="skip the 128 x 2^20 and uneven-batch extra keys")
     ap.add_argument("--workload", default="commit",
-                    choices=["commit", "uneven", "serve", "profile", "ef", "queries", "probe"],
+                    choices=["commit", "uneven", "serve", "profile", "ef", "queries", "probe", "fused-trace"],
                     help="commit: the contract line; others print their own JSON")
     ap.add_argument("--log-n", type=int, default=18, help="rows of the profile case (log2)")
     ap.add_argument("--cols", type=int, default=176, help="columns of the profile case")
@@ -883,7 +915,7 @@ def main():
     args = ap.parse_args()
     if args.workload != "commit":
         {"uneven": run_uneven, "serve": run_serve, "profile": run_profile_case, "ef": run_ef,
-         "queries": run_queries, "probe": run_probe}[args.workload](args)
+         "queries": run_queries, "probe": run_probe, "fused-trace": run_fused_trace}[args.workload](args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -182,6 +182,15 @@ glc_status glc_commit_batch(const glc_commit_job *jobs, uint32_t n_jobs, uint32_
  * No counterpart in the reference, whose per-call form launches one kernel per NTT stage
  * (log_n < 16) and per tree layer (crates/boojum-cuda/src/ntt.rs:201-241, src/poseidon2.rs:276-295). */
 glc_status glc_commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs, void *stream);
+/* glc_commit_batch_fused with a per-item trace: item i of the launch (items are numbered in
+ * stage order, heaviest first within a stage) writes trace[4i .. 4i+3] = {the GPU global timer
+ * in ns when its CTA claimed it, when its producers were done and it started, when it ended,
+ * (SM id << 40) | (CTA index << 8) | kind}, kind 0 NTT tile, 1 bit reversal, 2 leaves, 3 nodes,
+ * 4 cap entries.  Items from trace_items on are not recorded; the caller clears the buffer (a
+ * device buffer of 4 * trace_items words) to tell unwritten records apart.  No counterpart in the
+ * reference (its tracing is NVTX ranges around whole calls, shivini test.rs:2155-2181). */
+glc_status glc_commit_batch_fused_traced(const glc_commit_job *jobs, uint32_t n_jobs, uint64_t *trace,
+                                         uint64_t trace_items, void *stream);
 /* Waits of glc_commit_batch_fused that expired on the current device since the library was
  * loaded (0 unless something is wrong; a launch with an expired wait computes wrong results).
  * Synchronous. */

@@ -113,6 +113,36 @@ def test_commit_batch_fused_many_jobs(glc, syn):
     assert glc.commit.fused_timeouts() == 0
 
 
+def test_commit_batch_fused_traced(glc, oracle, syn):
+    """The traced fused launch gives the oracle's commitments, and its trace is consistent: one
+    record per item up to the buffer's size (the rest stays zero), claim <= start <= end, every
+    item kind present, leaves starting after the first NTT tile and caps ending last."""
+    import torch
+    shapes = [(12, 8, 1, 4, True), (14, 24, 2, 4, False), (16, 16, 1, 4, False), (9, 3, 0, 2, True)]
+    jobs = [make_job(glc, syn, l, c, e, cap, "ftrace-%d" % i, keep_monomials=m)
+            for i, (l, c, e, cap, m) in enumerate(shapes)]
+    trace = torch.zeros(4 << 16, dtype=torch.int64, device="cuda")
+    glc.commit.commit_batch_fused([j for j, _ in jobs], trace=trace)
+    for j, ev in jobs:
+        check_job(oracle, j, ev)
+    r = trace.cpu().numpy().view(np.uint64).reshape(-1, 4)
+    n = int((r[:, 2] > 0).sum())
+    assert 0 < n < len(r) and (r[n:] == 0).all() and (r[:n, 2] > 0).all()
+    r = r[:n]
+    assert (r[:, 0] <= r[:, 1]).all() and (r[:, 1] <= r[:, 2]).all()
+    kinds = r[:, 3] & np.uint64(0xFF)
+    assert set(kinds.tolist()) == {0, 1, 2, 3, 4}
+    assert r[kinds == 2, 1].min() > r[kinds == 0, 1].min()
+    assert r[kinds == 4, 2].max() == r[:, 2].max()
+    s = glc.commit.fused_trace_summary(r)
+    assert s["items"] == n and s["leaves"]["work_cta_ms"] > 0
+    # a buffer smaller than the launch keeps only the first items
+    small = torch.zeros(4 * 10, dtype=torch.int64, device="cuda")
+    glc.commit.commit_batch_fused([j for j, _ in jobs], trace=small)
+    assert (small.cpu().numpy().reshape(-1, 4)[:, 2] != 0).all()
+    assert glc.commit.fused_timeouts() == 0
+
+
 def test_commit_batch_fused_contract(glc, syn):
     job, _ = make_job(glc, syn, 17, 1, 1, 4, "fused-big")
     with pytest.raises(glc.GlcError):

@@ -56,6 +56,7 @@ SIGNATURES = {
     "glc_launch_count": (C.c_uint64, []),
     "glc_commit_batch": (C.c_int, [vp, u32, u32, vp]),
     "glc_commit_batch_fused": (C.c_int, [vp, u32, vp]),
+    "glc_commit_batch_fused_traced": (C.c_int, [vp, u32, u64p, u64, vp]),
     "glc_commit_batch_fused_timeouts": (C.c_int, [vp]),
     "glc_commit_graph_create": (C.c_int, [vp, u32, u32, vp]),
     "glc_commit_graph_launch": (C.c_int, [vp, vp]),

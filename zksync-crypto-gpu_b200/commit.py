@@ -75,12 +75,50 @@ def commit_batch(jobs: list[CommitJob], n_streams: int = 0, stream=None) -> None
     call("glc_commit_batch", C.addressof(arr) if jobs else None, len(jobs), n_streams, stream_handle(stream))
 
 
-def commit_batch_fused(jobs: list[CommitJob], stream=None) -> None:
+def commit_batch_fused(jobs: list[CommitJob], stream=None, trace=None) -> None:
     """Many small commitments (2^log_n <= 2^16 rows each) in ONE persistent launch
     (glc_commit_batch_fused): work items of every stage of every job, each waiting only for the
-    items it reads from."""
+    items it reads from.  `trace`: a device buffer of 4 * N 8-byte words, cleared by the caller,
+    that receives the per-item records of the first N items (glc_commit_batch_fused_traced; see
+    fused_trace_summary)."""
     arr = _array(jobs)
-    call("glc_commit_batch_fused", C.addressof(arr) if jobs else None, len(jobs), stream_handle(stream))
+    if trace is None:
+        call("glc_commit_batch_fused", C.addressof(arr) if jobs else None, len(jobs), stream_handle(stream))
+    else:
+        tp, tl = as_slice(trace)
+        call("glc_commit_batch_fused_traced", C.addressof(arr) if jobs else None, len(jobs), tp, tl // 4,
+             stream_handle(stream))
+
+
+FUSED_KINDS = ("ntt", "bitrev", "leaves", "nodes", "caps")
+
+
+def fused_trace_summary(records) -> dict:
+    """Where the CTAs of one fused launch spent their time, from its trace (an (n, 4) array of
+    uint64 records as glc_commit_batch_fused_traced writes them; all-zero rows are unwritten).
+    Per item kind: items, CTA-milliseconds of work (start -> end) and of waiting (claim -> start:
+    entry search and producers), first start and last end (ms from the first claim); the
+    CTA-milliseconds between one item's end and the same CTA's next claim; and the launch span."""
+    import numpy as np
+    r = np.asarray(records, dtype=np.uint64).reshape(-1, 4)
+    r = r[r[:, 2] > 0].astype(np.int64)
+    if len(r) == 0:
+        return {"items": 0}
+    t00 = r[:, 0].min()
+    claim, start, end = (r[:, 0] - t00) / 1e6, (r[:, 1] - t00) / 1e6, (r[:, 2] - t00) / 1e6
+    kind, cta = r[:, 3] & 0xFF, (r[:, 3] >> 8) & 0xFFFFFFFF
+    out = {"items": int(len(r)), "ctas": int(len(np.unique(cta))), "span_ms": float(end.max())}
+    for k, name in enumerate(FUSED_KINDS):
+        m = kind == k
+        if m.any():
+            out[name] = {"items": int(m.sum()), "work_cta_ms": float((end - start)[m].sum()),
+                         "wait_cta_ms": float((start - claim)[m].sum()), "first_start_ms": float(start[m].min()),
+                         "last_end_ms": float(end[m].max())}
+    order = np.lexsort((claim, cta))
+    same = cta[order][1:] == cta[order][:-1]
+    out["between_items_cta_ms"] = float((claim[order][1:] - end[order][:-1])[same].sum())
+    out["cta_ms_total"] = float(out["ctas"] * end.max())
+    return out
 
 
 def fused_timeouts() -> int:

@@ -82,11 +82,24 @@ __device__ __forceinline__ void red_release_add(uint32_t *p, uint32_t v) {
   asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Trace timestamps: the GPU's global nanosecond timer (one clock for every SM).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ uint32_t sm_id() {
+  uint32_t v;
+  asm("mov.u32 %0, %%smid;" : "=r"(v));
+  return v;
+}
+
 static constexpr uint32_t FUSED_WAIT_LIMIT = 1u << 22;  // x 200 ns sleeps: about 1 s
 
 __global__ void __launch_bounds__(FUSED_THREADS, 3)
     fused_commit_kernel(const FusedEntry *entries, uint32_t n_entries, uint64_t total_units, uint32_t *counters,
-                        uint32_t *abort_flag, unsigned long long *next_unit) {
+                        uint32_t *abort_flag, unsigned long long *next_unit, unsigned long long *trace,
+                        uint64_t trace_items) {
   extern __shared__ uint64_t smem[];
   __shared__ uint64_t s_unit;
   __shared__ uint32_t s_entry;
@@ -106,6 +119,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 3)
     __syncthreads();
     const uint64_t u = s_unit;
     if (u >= total_units) break;
+    const unsigned long long t_claim = (trace && tid == 0) ? global_ns() : 0ull;
     // the entry holding item u, the last one whose first item is <= u: a 32-way search by warp 0
     // (three rounds of dependent loads for up to 32K entries)
     if (tid < 32) {
@@ -137,6 +151,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 3)
       }
     }
     __syncthreads();  // the acquire above orders the producers' writes before this CTA's reads
+    const unsigned long long t_start = (trace && tid == 0) ? global_ns() : 0ull;
     const uint64_t local = u - E.first;
     const uint32_t kind = E.kind;
     if (kind == FK_NTT) {
@@ -178,6 +193,13 @@ __global__ void __launch_bounds__(FUSED_THREADS, 3)
     }
     __syncthreads();  // every thread's writes of this item precede the release below
     if (tid == 0) {
+      if (trace && u < trace_items) {
+        unsigned long long *r = trace + 4 * u;
+        r[0] = t_claim;
+        r[1] = t_start;
+        r[2] = global_ns();
+        r[3] = ((unsigned long long)sm_id() << 40) | ((unsigned long long)blockIdx.x << 8) | E.kind;
+      }
       if (E.done1 != NO_COUNTER) red_release_add(counters + E.done1, 1u);
       if (E.done2 != NO_COUNTER) red_release_add(counters + E.done2, 1u);
     }
@@ -448,7 +470,8 @@ void fused_forget_device(int dev) {
 
 using namespace glc;
 
-extern "C" glc_status glc_commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs, void *stream_) {
+static glc_status commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs, unsigned long long *trace,
+                                     uint64_t trace_items, void *stream_) {
   if (n_jobs == 0) return 0;
   if (!jobs) return fail("commit_batch_fused: null jobs");
   for (uint32_t i = 0; i < n_jobs; i++) {
@@ -490,13 +513,24 @@ extern "C" glc_status glc_commit_batch_fused(const glc_commit_job *jobs, uint32_
     unsigned long long *next = reinterpret_cast<unsigned long long *>(buf + eb + cb - sizeof(unsigned long long));
     uint32_t ne = (uint32_t)P.entries.size();
     uint64_t tu = total;
-    void *args[] = {(void *)&de, (void *)&ne, (void *)&tu, (void *)&counters, (void *)&abort_flag, (void *)&next};
+    void *args[] = {(void *)&de,   (void *)&ne,   (void *)&tu,         (void *)&counters, (void *)&abort_flag,
+                    (void *)&next, (void *)&trace, (void *)&trace_items};
     ce = cudaLaunchCooperativeKernel((const void *)fused_commit_kernel, dim3((unsigned)(per_sm * sms)),
                                      dim3(FUSED_THREADS), args, P.smem, stream);
     count_launches(1);
   }
   const cudaError_t fe = cudaFreeAsync(buf, stream);
   return (int)(ce != cudaSuccess ? ce : fe);
+}
+
+extern "C" glc_status glc_commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs, void *stream) {
+  return commit_batch_fused(jobs, n_jobs, nullptr, 0, stream);
+}
+
+extern "C" glc_status glc_commit_batch_fused_traced(const glc_commit_job *jobs, uint32_t n_jobs, uint64_t *trace,
+                                                    uint64_t trace_items, void *stream) {
+  if (!trace && trace_items) return fail("commit_batch_fused_traced: null trace buffer");
+  return commit_batch_fused(jobs, n_jobs, reinterpret_cast<unsigned long long *>(trace), trace_items, stream);
 }
 
 extern "C" glc_status glc_commit_batch_fused_timeouts(uint64_t *out) {

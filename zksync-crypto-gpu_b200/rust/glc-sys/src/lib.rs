@@ -158,6 +158,8 @@ extern "C" {
         log_cap: u32, cap: *mut u64, stream: Stream) -> GlcStatus;
     pub fn glc_commit_batch(jobs: *const glc_commit_job, n_jobs: u32, n_streams: u32, stream: Stream) -> GlcStatus;
     pub fn glc_commit_batch_fused(jobs: *const glc_commit_job, n_jobs: u32, stream: Stream) -> GlcStatus;
+    pub fn glc_commit_batch_fused_traced(jobs: *const glc_commit_job, n_jobs: u32, trace: *mut u64,
+        trace_items: u64, stream: Stream) -> GlcStatus;
     pub fn glc_commit_batch_fused_timeouts(out: *mut u64) -> GlcStatus;
     pub fn glc_commit_graph_create(jobs: *const glc_commit_job, n_jobs: u32, n_streams: u32,
         out: *mut *mut glc_graph) -> GlcStatus;
