@@ -793,6 +793,85 @@ def run_ef(args):
     ctx.destroy()
 
 
+def run_witness(args):
+    """Witness-to-trace fill of the large commitment's trace: 2^22 rows (--witness-log-rows) x 176 columns (150
+    variable, 25 witness, 1 multiplicity) gathered from 2^28 witness values by seeded random u32
+    indexes (3% placeholders), multiplicities for 3/4 of the rows.  HBM-bound gather: per element
+    4 bytes of index and 8 of value read, 8 written (algorithmic); the value read is a separate
+    32-byte DRAM sector at random indexes.  Also the reference's select kernel on the same indexes,
+    compared element for element."""
+    glc, torch, ctx = _setup_device()
+    syn = importlib.import_module("zksync-crypto-gpu_b200.synthetic")
+    log_n, nv, nw, nm = args.witness_log_rows, 150, 25, 1
+    n = 1 << log_n
+    n_values = 1 << 28
+    values = torch.empty(n_values, dtype=torch.int64, device="cuda")
+    syn.fill_device(values, "witness-values")
+    gen = torch.Generator(device="cuda").manual_seed(17)
+    def indexes(count):
+        ix = torch.randint(0, n_values, (count,), generator=gen, device="cuda", dtype=torch.int64)
+        ph = torch.rand(count, generator=gen, device="cuda") < 0.03
+        return (ix | (ph.to(torch.int64) << 31)).to(torch.int32)
+    vi, wi = indexes(nv * n), indexes(nw * n)
+    mult = torch.randint(0, 1 << 20, (3 * n // 4,), generator=gen, device="cuda", dtype=torch.int32)
+    trace = torch.empty((nv + nw + nm) * n, dtype=torch.int64, device="cuda")
+    fill = lambda: glc.trace.fill_from_remote_witness_data(vi, wi, values, mult, trace, nv, nw, nm, n)
+    peaks, kind = measured_peaks()
+    for _ in range(max(args.warmup, 1)):
+        fill()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        fill()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    elems = (nv + nw + nm) * n
+    gathered = (nv + nw) * n
+    alg = 20 * gathered + 12 * n * nm
+    sectors = (4 + 32 + 8) * gathered + 12 * n * nm
+    out = {"workload": "witness-to-trace fill: 2^%d rows x 176 columns (150 variable, 25 witness, 1 multiplicity) "
+                       "from 2^28 values, random indexes, 3%% placeholders" % log_n,
+           "ms": ms, "elements_per_s": elems / (ms / 1e3), "algorithmic_gbs": alg / (ms / 1e3) / 1e9,
+           "sector_gbs": sectors / (ms / 1e3) / 1e9, "hbm_gbs_peak": peaks["hbm_gbs"], "peak_source": kind,
+           "frac_sector_traffic_of_hbm": sectors / (ms / 1e3) / 1e9 / peaks["hbm_gbs"]}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import refkern
+        have_ref = refkern.available()
+    except Exception:
+        have_ref = False
+    if have_ref:
+        ref = torch.empty_like(trace)
+        s_ = torch.cuda.current_stream().cuda_stream
+        def ref_fill():
+            refkern.call("ref_select", vi.data_ptr(), values.data_ptr(), ref.data_ptr(), nv * n, s_)
+            refkern.call("ref_select", wi.data_ptr(), values.data_ptr(), ref.data_ptr() + 8 * nv * n, nw * n, s_)
+        ref_fill()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            ref_fill()
+        e1.record()
+        torch.cuda.synchronize()
+        rms = e0.elapsed_time(e1) / args.steps
+        out["reference_select_kernel"] = {"ms_for_the_selects": rms, "speedup_of_the_selects": None,
+                                          "parity": bool((ref[:gathered] == trace[:gathered]).all())}
+        # this build's selects alone (the multiplicity column is not part of the reference kernel)
+        e0.record()
+        for _ in range(args.steps):
+            glc.ops_complex.select(vi, values, trace[:nv * n])
+            glc.ops_complex.select(wi, values, trace[nv * n:gathered])
+        e1.record()
+        torch.cuda.synchronize()
+        ours = e0.elapsed_time(e1) / args.steps
+        out["reference_select_kernel"]["speedup_of_the_selects"] = rms / ours
+        out["selects_ms"] = ours
+    print(json.dumps(out), flush=True)
+    ctx.destroy()
+
+
 def run_queries(args):
     """Query openings on the 128 x 2^20 commitment (LDE x2, cap 16): for 100 seeded query indexes
     of one coset, gather the 100 rows of the 128 LDE columns (gather_rows) and the 17-layer Merkle
@@ -902,11 +981,13 @@ def main():
     ap.add_argument("--no-ref-kernels", action="store_true", help="skip the reference-kernel timing and parity leg")
     ap.add_argument("--no-extras", action="store_true", help="skip the 128 x 2^20 and uneven-batch extra keys")
     ap.add_argument("--workload", default="commit",
-                    choices=["commit", "uneven", "serve", "profile", "ef", "queries", "probe", "fused-trace"],
+                    choices=["commit", "uneven", "serve", "profile", "ef", "queries", "probe", "fused-trace",
+                             "witness"],
                     help="commit: the contract line; others print their own JSON")
     ap.add_argument("--log-n", type=int, default=18, help="rows of the profile case (log2)")
     ap.add_argument("--cols", type=int, default=176, help="columns of the profile case")
     ap.add_argument("--ef-log-rows", type=int, default=22, help="rows of the extension-layout workload (log2)")
+    ap.add_argument("--witness-log-rows", type=int, default=22, help="rows of the witness-fill workload (log2)")
     ap.add_argument("--streams", type=int, default=8)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-jobs", type=int, default=400)
@@ -915,7 +996,8 @@ def main():
     args = ap.parse_args()
     if args.workload != "commit":
         {"uneven": run_uneven, "serve": run_serve, "profile": run_profile_case, "ef": run_ef,
-         "queries": run_queries, "probe": run_probe, "fused-trace": run_fused_trace}[args.workload](args)
+         "queries": run_queries, "probe": run_probe, "fused-trace": run_fused_trace,
+         "witness": run_witness}[args.workload](args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -122,6 +122,29 @@ glc_status glc_ef_vectorized_to_tuples(const uint64_t *src, uint64_t src_stride,
 glc_status glc_ef_tuples_to_vectorized(const uint64_t *src, uint64_t src_stride, uint64_t *dst, uint64_t dst_stride,
                                        uint32_t rows, uint32_t cols, void *stream);
 
+/* ops_complex::select (crates/boojum-cuda/src/ops_complex.rs:446-463, kernel native/ops_complex.cu:
+ * 158-164): dst[i] = indexes[i] has bit 31 set ? 0 : src[indexes[i]] for i < indexes_len.  Every
+ * length must fit in 32 bits and dst must hold indexes_len elements.  An index at or past src_len
+ * (other than a placeholder) yields 0 (the reference reads whatever lies there). */
+glc_status glc_select(const uint32_t *indexes, uint64_t indexes_len, const uint64_t *src, uint64_t src_len,
+                      uint64_t *dst, uint64_t dst_len, void *stream);
+
+/* GenericTraceStorage::fill_from_remote_witness_data (crates/shivini/src/data_structures/trace.rs:
+ * 108-193): the trace matrix of a commitment from the witness values, column-major with
+ * domain_size rows: num_variable_cols columns selected by variable_indexes, then num_witness_cols
+ * columns selected by witness_indexes (glc_select on `values`), then num_multiplicity_cols (0 or 1)
+ * column of the lookup multiplicities (u32, as field elements) zero-padded to domain_size.  Same
+ * checks as the reference: variable_indexes_len = num_variable_cols * domain_size,
+ * witness_indexes_len = num_witness_cols * domain_size, trace_len = columns * domain_size,
+ * multiplicities_len <= domain_size.  All buffers are device buffers (the reference copies the
+ * values and multiplicities from the host first). */
+glc_status glc_trace_fill_from_witness(const uint32_t *variable_indexes, uint64_t variable_indexes_len,
+                                       const uint32_t *witness_indexes, uint64_t witness_indexes_len,
+                                       const uint64_t *values, uint64_t values_len, const uint32_t *multiplicities,
+                                       uint64_t multiplicities_len, uint64_t *trace, uint64_t trace_len,
+                                       uint32_t num_variable_cols, uint32_t num_witness_cols,
+                                       uint32_t num_multiplicity_cols, uint64_t domain_size, void *stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Commitment jobs (no single counterpart in boojum-cuda: this is the sequence shivini runs for one
  * trace / argument / quotient commitment, crates/shivini/src/data_structures/storage.rs:155-330,

@@ -286,6 +286,25 @@ void or_ef_tuples_to_vectorized(const uint64_t *t, uint64_t t_stride, uint64_t *
     }
 }
 
+/* ---- witness-to-trace fill (ops_complex.cu:158-164; shivini trace.rs:108-193, cs/witness.rs:6-31) ---- */
+void or_select(const uint32_t *indexes, uint64_t count, const uint64_t *src, uint64_t src_len, uint64_t *dst) {
+  for (uint64_t i = 0; i < count; i++) {
+    const uint32_t ix = indexes[i];
+    dst[i] = (ix & 0x80000000u) || ix >= src_len ? 0 : src[ix];
+  }
+}
+
+void or_trace_fill(const uint32_t *variable_indexes, const uint32_t *witness_indexes, const uint64_t *values,
+                   uint64_t values_len, const uint32_t *multiplicities, uint64_t multiplicities_len, uint64_t *trace,
+                   uint32_t nv, uint32_t nw, uint32_t nm, uint64_t n) {
+  or_select(variable_indexes, (uint64_t)nv * n, values, values_len, trace);
+  or_select(witness_indexes, (uint64_t)nw * n, values, values_len, trace + (uint64_t)nv * n);
+  if (nm) {
+    uint64_t *m = trace + (uint64_t)(nv + nw) * n;
+    for (uint64_t i = 0; i < n; i++) m[i] = i < multiplicities_len ? (uint64_t)multiplicities[i] : 0;
+  }
+}
+
 /* ------------------------------------------------------------------------------------------
  * Poseidon2 over Goldilocks, width 12, rate 8, capacity 4, x^7, 4+4 full and 22 partial
  * rounds (crates/boojum-cuda/native/poseidon2/gl/poseidon2_gl_st.cu:9-23,

@@ -102,6 +102,17 @@ void or_ef_vectorized_to_tuples(const uint64_t *v, uint64_t v_stride, uint64_t *
 void or_ef_tuples_to_vectorized(const uint64_t *t, uint64_t t_stride, uint64_t *v, uint64_t v_stride, uint32_t rows,
                                 uint32_t cols);
 
+/* ops_complex::select (native/ops_complex.cu:158-164): dst[i] = indexes[i] has bit 31 set ? 0 :
+ * src[indexes[i]].  An index at or past src_len reads as 0 (the library's defined behaviour for
+ * what the reference leaves unchecked). */
+void or_select(const uint32_t *indexes, uint64_t count, const uint64_t *src, uint64_t src_len, uint64_t *dst);
+/* GenericTraceStorage::fill_from_remote_witness_data (crates/shivini/src/data_structures/
+ * trace.rs:108-193): nv variable columns and nw witness columns selected from `values`, then nm
+ * (0 or 1) columns of multiplicities zero-padded to n rows; trace is (nv + nw + nm) x n. */
+void or_trace_fill(const uint32_t *variable_indexes, const uint32_t *witness_indexes, const uint64_t *values,
+                   uint64_t values_len, const uint32_t *multiplicities, uint64_t multiplicities_len, uint64_t *trace,
+                   uint32_t nv, uint32_t nw, uint32_t nm, uint64_t n);
+
 int or_commit(const uint64_t *evals, uint32_t log_n, uint32_t cols, uint32_t log_lde, uint32_t log_cap,
               uint64_t *monomials_out, uint64_t *lde_out, uint64_t *trees_out, uint64_t *cap_out, int threads);
 

@@ -52,6 +52,9 @@ def lib():
         L.or_p2_gather_merkle_paths.argtypes = [u32p, C.c_uint32, u64p, sz, C.c_uint32, u64p, sz]
         L.or_p2_find_opening.restype = C.c_int64
         L.or_p2_find_opening.argtypes = [u64p, C.c_uint32, u64p, C.c_uint32, u64p, C.c_uint32]
+        L.or_select.argtypes = [u32p, C.c_uint64, u64p, C.c_uint64, u64p]
+        L.or_trace_fill.argtypes = [u32p, u32p, u64p, C.c_uint64, u32p, C.c_uint64, u64p, C.c_uint32, C.c_uint32,
+                                    C.c_uint32, C.c_uint64]
         L.or_commit.argtypes = [u64p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u64p, u64p, u64p, u64p, C.c_int]
         _lib = L
     return _lib
@@ -125,6 +128,27 @@ def ef_tuples_to_vectorized(t, t_stride, rows, cols, v_stride=None):
     v = np.zeros(2 * cols * v_stride, dtype=np.uint64)
     lib().or_ef_tuples_to_vectorized(_p(t), t_stride, _p(v), v_stride, rows, cols)
     return v
+
+
+def select(indexes, src):
+    """ops_complex::select: src[indexes[i]], 0 where bit 31 is set (or the index is past src)."""
+    idx = np.ascontiguousarray(indexes, dtype=np.uint32)
+    src = np.ascontiguousarray(src, dtype=np.uint64)
+    out = np.zeros(idx.size, dtype=np.uint64)
+    lib().or_select(_p32(idx), idx.size, _p(src), src.size, _p(out))
+    return out
+
+
+def trace_fill(variable_indexes, witness_indexes, values, multiplicities, nv, nw, nm, n):
+    """fill_from_remote_witness_data: the (nv + nw + nm) x n trace."""
+    vi = np.ascontiguousarray(variable_indexes, dtype=np.uint32)
+    wi = np.ascontiguousarray(witness_indexes if witness_indexes is not None else [], dtype=np.uint32)
+    vals = np.ascontiguousarray(values, dtype=np.uint64)
+    mult = np.ascontiguousarray(multiplicities if multiplicities is not None else [], dtype=np.uint32)
+    assert vi.size == nv * n and wi.size == nw * n and nm <= 1 and mult.size <= n * nm
+    out = np.zeros((nv + nw + nm) * n, dtype=np.uint64)
+    lib().or_trace_fill(_p32(vi), _p32(wi), _p(vals), vals.size, _p32(mult), mult.size, _p(out), nv, nw, nm, n)
+    return out
 
 
 def leaves(values, results_len, log_rows_per_hash=0, load_intermediate=False, store_intermediate=False,

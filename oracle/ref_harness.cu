@@ -8,6 +8,7 @@
 //   - Context::create: table contents and the __constant__ descriptors (src/context.rs:171-282)
 //   - batch_ntt_internal: per-size kernel plans and launch shapes (src/ntt.rs:70-291)
 //   - launch_bit_reverse (src/ops_complex.rs:273-306)
+//   - select with get_launch_dims (src/ops_complex.rs:27-29, 446-463)
 //   - compute_leaf_hashes / compute_node_hashes / build_merkle_tree / gathers, with the
 //     st-or-mt kernel choice by wave count (src/poseidon2.rs:143-380)
 // Round constants for the Poseidon2 kernels are compiled in from a generated header
@@ -62,6 +63,7 @@ extern "C" __global__ void poseidon2_gl_mt_nodes_kernel(const uint64_t *, uint64
 extern "C" __global__ void poseidon2_gl_gather_rows_kernel(const unsigned *, unsigned, RefPtrStride, RefPtrStride);
 extern "C" __global__ void poseidon2_gl_gather_merkle_paths_kernel(const unsigned *, unsigned, const uint64_t *, unsigned,
                                                                    uint64_t *);
+extern "C" __global__ void select_kernel(const unsigned *, const uint64_t *, uint64_t *, unsigned);
 
 namespace {
 
@@ -360,5 +362,15 @@ extern "C" int ref_p2_gather_merkle_paths(const unsigned *indexes, unsigned inde
   if (bx == 0 || layers_count == 0) return 0;
   poseidon2_gl_gather_merkle_paths_kernel<<<dim3((indexes_count + bx - 1) / bx, 4, layers_count), bx, 0, stream>>>(
       indexes, indexes_count, values, log_leaves, results);
+  return (int)cudaGetLastError();
+}
+
+// ops_complex::select (src/ops_complex.rs:446-463): one thread per index, get_launch_dims = 128
+// threads per block (WARP_SIZE * 4, ops_complex.rs:27-29).
+extern "C" int ref_select(const unsigned *indexes, const uint64_t *src, uint64_t *dst, unsigned count,
+                          cudaStream_t stream) {
+  if (count == 0) return 0;
+  const unsigned block = count < 128 ? count : 128;
+  select_kernel<<<(count + block - 1) / block, block, 0, stream>>>(indexes, src, dst, count);
   return (int)cudaGetLastError();
 }

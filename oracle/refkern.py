@@ -30,6 +30,7 @@ def lib():
             "ref_p2_build_merkle_tree": [vp, sz, vp, sz, u32, u32, vp],
             "ref_p2_gather_rows": [vp, u32, u32, vp, sz, vp, sz, u32, vp],
             "ref_p2_gather_merkle_paths": [vp, u32, vp, sz, vp, u32, vp],
+            "ref_select": [vp, vp, vp, u32, vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)

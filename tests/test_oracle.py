@@ -260,3 +260,22 @@ def test_extension_layouts(oracle):
     assert t.tolist() == want
     back = oracle.ef_tuples_to_vectorized(t, 5, 5, 3, 7).reshape(6, 7)
     assert (back[:, :5] == v.reshape(6, 7)[:, :5]).all() and (back[:, 5:] == 0).all()
+
+
+def test_select_and_trace_fill(oracle):
+    """select: src[index], 0 for a placeholder (bit 31) or an index past the source; the trace fill
+    is the variable selects, the witness selects and the zero-padded multiplicities, in that order
+    (ops_complex.cu:158-164, trace.rs:108-193), restated here in numpy."""
+    rng = np.random.default_rng(3)
+    src = rng.integers(0, 2**64, size=300, dtype=np.uint64)
+    ix = rng.integers(0, 350, size=4000, dtype=np.uint32)
+    ix[::9] |= np.uint32(1 << 31)
+    sel = lambda i: np.where(((i >> 31) == 0) & (i < src.size), src[np.minimum(i & 0x7FFFFFFF, src.size - 1)], 0)
+    assert (oracle.select(ix, src) == sel(ix)).all()
+    n, nv, nw = 64, 3, 2
+    vi, wi = ix[:nv * n], ix[nv * n:(nv + nw) * n]
+    mult = rng.integers(0, 2**32, size=40, dtype=np.uint32)
+    got = oracle.trace_fill(vi, wi, src, mult, nv, nw, 1, n)
+    want = np.concatenate([sel(vi), sel(wi), mult.astype(np.uint64), np.zeros(n - 40, np.uint64)])
+    assert (got == want).all()
+    assert (oracle.trace_fill(vi, None, src, None, nv, 0, 0, n) == sel(vi)).all()

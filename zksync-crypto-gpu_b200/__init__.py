@@ -12,10 +12,10 @@ from ._lib import GlcError, LIB_PATH
 
 _lib.lib()  # load libglc.so now: fail loudly at import when it is not built
 
-from . import commit, context, extension_field, ntt, ops_complex, poseidon2, serve, tuning  # noqa: E402
+from . import commit, context, extension_field, ntt, ops_complex, poseidon2, serve, trace, tuning  # noqa: E402
 from .commit import CommitGraph, CommitJob  # noqa: E402
 from .context import Context  # noqa: E402
 from .poseidon2 import GLHasher  # noqa: E402
 
 __all__ = ["Context", "GLHasher", "GlcError", "DevicePtr", "LIB_PATH", "CommitJob", "CommitGraph", "commit",
-           "context", "extension_field", "ntt", "ops_complex", "poseidon2", "serve", "tuning"]
+           "context", "extension_field", "ntt", "ops_complex", "poseidon2", "serve", "trace", "tuning"]

@@ -50,6 +50,8 @@ SIGNATURES = {
     "glc_poseidon2_gather_merkle_paths": (C.c_int, [u32p, sz, u64p, sz, u64p, sz, u32, vp]),
     "glc_ef_vectorized_to_tuples": (C.c_int, [u64p, u64, u64p, u64, u32, u32, vp]),
     "glc_ef_tuples_to_vectorized": (C.c_int, [u64p, u64, u64p, u64, u32, u32, vp]),
+    "glc_select": (C.c_int, [u32p, u64, u64p, u64, u64p, u64, vp]),
+    "glc_trace_fill_from_witness": (C.c_int, [u32p, u64, u32p, u64, u64p, u64, u32p, u64, u64p, u64, u32, u32, u32, u64, vp]),
     "glc_commit": (C.c_int, [vp, vp]),
     "glc_commit_profiled": (C.c_int, [vp, vp, vp, u32]),
     "glc_commit_cap_noalloc": (C.c_int, [u64p, u64, u32, u32, u32, u32, u64p, vp]),

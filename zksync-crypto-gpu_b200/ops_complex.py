@@ -1,6 +1,7 @@
-"""Row bit reversal of column-major matrices: the counterpart of boojum-cuda's
-ops_complex::bit_reverse / bit_reverse_in_place (crates/boojum-cuda/src/ops_complex.rs:309-331).
-A matrix is given as (buffer, rows, cols, stride) like the reference's DeviceMatrixChunk."""
+"""Row bit reversal of column-major matrices and the index gather: the counterparts of boojum-cuda's
+ops_complex::bit_reverse / bit_reverse_in_place (crates/boojum-cuda/src/ops_complex.rs:309-331)
+and ops_complex::select (ops_complex.rs:446-463).  A matrix is given as (buffer, rows, cols,
+stride) like the reference's DeviceMatrixChunk."""
 from __future__ import annotations
 
 from ._buffers import as_slice, stream_handle
@@ -24,3 +25,13 @@ def bit_reverse_in_place(values, rows: int, cols: int, stride: int | None = None
     if cols and vl < (cols - 1) * stride + rows:
         raise ValueError("bit_reverse_in_place: buffer shorter than the matrix")
     call("glc_bit_reverse_in_place", vp_, stride, rows, cols, stream_handle(stream))
+
+
+def select(indexes, src, dst, stream=None) -> None:
+    """ops_complex::select (ops_complex.rs:446-463): dst[i] = src[indexes[i]] for i < len(indexes),
+    0 where bit 31 of the index is set.  `indexes`: a device buffer of 4-byte elements (a torch
+    int32 tensor holds the u32 bit patterns)."""
+    ip, il = as_slice(indexes, 4)
+    sp, sl = as_slice(src)
+    dp, dl = as_slice(dst)
+    call("glc_select", ip, il, sp, sl, dp, dl, stream_handle(stream))

@@ -1,7 +1,7 @@
 //! boojum-cuda's commitment-path entry points with their reference signatures, implemented over
 //! libglc.  The bodies of crates/boojum-cuda/src/ntt.rs:294-369 (batch NTTs),
-//! src/poseidon2.rs:180-380 (GpuTreeHasher for GLHasher), src/ops_complex.rs:309-331 (bit
-//! reversal) and src/context.rs:171-297 (Context) become calls into libglc; the contract checks
+//! src/poseidon2.rs:180-380 (GpuTreeHasher for GLHasher), src/ops_complex.rs:309-331 and 446-463
+//! (bit reversal, select) and src/context.rs:171-297 (Context) become calls into libglc; the contract checks
 //! stay the reference's `assert!`s, so a caller sees the same panics, and libglc re-checks them
 //! (returning cudaErrorInvalidValue).  shivini switches by importing these paths instead of
 //! boojum_cuda's.
@@ -36,6 +36,8 @@ mod ffi {
             cols: u32, stream: cudaStream_t) -> CudaError;
         pub fn glc_bit_reverse_in_place(values: *mut GL, stride: u64, rows: u32, cols: u32,
             stream: cudaStream_t) -> CudaError;
+        pub fn glc_select(indexes: *const u32, indexes_len: u64, src: *const GL, src_len: u64, dst: *mut GL,
+            dst_len: u64, stream: cudaStream_t) -> CudaError;
         pub fn glc_poseidon2_set_round_constants(round_constants: *const u64) -> CudaError;
         pub fn glc_poseidon2_compute_leaf_hashes(values: *const GL, values_len: usize, results: *mut GL,
             results_len: usize, log_rows_per_hash: u32, load_intermediate: bool, store_intermediate: bool,
@@ -150,6 +152,20 @@ pub mod ops_complex {
         assert!(values.len() >= (cols - 1) * stride + rows);
         unsafe { ffi::glc_bit_reverse_in_place(values.as_mut_ptr(), stride as u64, rows as u32, cols as u32, stream.into()) }
             .wrap()
+    }
+
+    /// ops_complex::select (crates/boojum-cuda/src/ops_complex.rs:446-463): dst[i] = src[indexes[i]],
+    /// or zero where bit 31 of the index is set.
+    pub fn select(indexes: &DeviceSlice<u32>, src: &DeviceSlice<GL>, dst: &mut DeviceSlice<GL>, stream: &CudaStream)
+        -> CudaResult<()> {
+        assert!(indexes.len() <= u32::MAX as usize);
+        assert!(src.len() <= u32::MAX as usize);
+        assert!(dst.len() <= u32::MAX as usize);
+        unsafe {
+            ffi::glc_select(indexes.as_ptr(), indexes.len() as u64, src.as_ptr(), src.len() as u64, dst.as_mut_ptr(),
+                dst.len() as u64, stream.into())
+        }
+        .wrap()
     }
 }
 

@@ -150,6 +150,15 @@ extern "C" {
     pub fn glc_ef_tuples_to_vectorized(src: *const u64, src_stride: u64, dst: *mut u64, dst_stride: u64, rows: u32,
         cols: u32, stream: Stream) -> GlcStatus;
 
+    // ops_complex::select (crates/boojum-cuda/src/ops_complex.rs:446-463) and shivini's
+    // fill_from_remote_witness_data (crates/shivini/src/data_structures/trace.rs:108-193)
+    pub fn glc_select(indexes: *const u32, indexes_len: u64, src: *const u64, src_len: u64, dst: *mut u64,
+        dst_len: u64, stream: Stream) -> GlcStatus;
+    pub fn glc_trace_fill_from_witness(variable_indexes: *const u32, variable_indexes_len: u64,
+        witness_indexes: *const u32, witness_indexes_len: u64, values: *const u64, values_len: u64,
+        multiplicities: *const u32, multiplicities_len: u64, trace: *mut u64, trace_len: u64, num_variable_cols: u32,
+        num_witness_cols: u32, num_multiplicity_cols: u32, domain_size: u64, stream: Stream) -> GlcStatus;
+
     // commitment jobs (shivini's per-commitment sequence as one call)
     pub fn glc_commit(job: *const glc_commit_job, stream: Stream) -> GlcStatus;
     pub fn glc_commit_profiled(job: *const glc_commit_job, stream: Stream, events: *mut *mut c_void,
