@@ -214,6 +214,20 @@ glc_status glc_commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs, v
  * reference (its tracing is NVTX ranges around whole calls, shivini test.rs:2155-2181). */
 glc_status glc_commit_batch_fused_traced(const glc_commit_job *jobs, uint32_t n_jobs, uint64_t *trace,
                                          uint64_t trace_items, void *stream);
+/* glc_commit_batch_fused that a host can stop: before each item (and every 64 polls while an item
+ * waits for its producers) the launch reads the 32-bit word at `cancel` (a device-readable
+ * address: a word from glc_mapped_word_create, or device memory).  Once it reads non-zero, no
+ * CTA claims or starts another item and every wait ends, so the launch returns after the items
+ * already running; the outputs are then incomplete.  If `status` is not null, the last CTA to
+ * leave writes 1 there when every item ran, 2 when the cancel skipped some.  A watchdog for the
+ * persistent grid; the reference has no persistent kernel and no counterpart. */
+glc_status glc_commit_batch_fused_cancellable(const glc_commit_job *jobs, uint32_t n_jobs, const uint32_t *cancel,
+                                              uint32_t *status, void *stream);
+/* A zeroed 32-bit word of page-locked host memory mapped into the device: the host reads and
+ * writes *host, kernels use *device (for glc_commit_batch_fused_cancellable's cancel and status).
+ * Released with glc_mapped_word_destroy(host). */
+glc_status glc_mapped_word_create(uint32_t **host, uint32_t **device);
+glc_status glc_mapped_word_destroy(uint32_t *host);
 /* Waits of glc_commit_batch_fused that expired on the current device since the library was
  * loaded (0 unless something is wrong; a launch with an expired wait computes wrong results).
  * Synchronous. */

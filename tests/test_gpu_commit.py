@@ -143,6 +143,65 @@ def test_commit_batch_fused_traced(glc, oracle, syn):
     assert glc.commit.fused_timeouts() == 0
 
 
+def test_commit_batch_fused_cancellable(glc, syn):
+    """The cancellable fused launch: never cancelled, it equals the plain fused launch and reports
+    1; cancelled before it starts, it runs no item (caps untouched) and reports 2; cancelled by the
+    host while it runs, it ends early (status 2) or had already finished (status 1).  Every later
+    launch is unaffected and no wait expires."""
+    import time
+    import torch
+    shapes = [(15, 128, 2, 4)] * 12 + [(13, 16, 1, 4)] * 8
+    jobs = [make_job(glc, syn, l, c, e, cap, "fcancel-%d" % i, keep_monomials=False)[0]
+            for i, (l, c, e, cap) in enumerate(shapes)]
+    glc.commit.commit_batch_fused(jobs)
+    want = [from_dev(j.cap).copy() for j in jobs]
+    cancel, status = glc.commit.MappedWord(), glc.commit.MappedWord()
+    # never cancelled
+    for j in jobs:
+        j.cap.zero_()
+    glc.commit.commit_batch_fused_cancellable(jobs, cancel, status)
+    torch.cuda.synchronize()
+    assert status.value == 1 and all((from_dev(j.cap) == w).all() for j, w in zip(jobs, want))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    glc.commit.commit_batch_fused_cancellable(jobs, cancel, status)
+    e1.record()
+    torch.cuda.synchronize()
+    full_ms = e0.elapsed_time(e1)
+    # cancelled before the launch: nothing runs
+    for j in jobs:
+        j.cap.zero_()
+    status.value = 0
+    cancel.value = 1
+    e0.record()
+    glc.commit.commit_batch_fused_cancellable(jobs, cancel, status)
+    e1.record()
+    torch.cuda.synchronize()
+    assert status.value == 2 and e0.elapsed_time(e1) < full_ms / 4
+    assert all((from_dev(j.cap) == 0).all() for j in jobs)
+    # cancelled while running
+    cancel.value = 0
+    status.value = 0
+    e0.record()
+    glc.commit.commit_batch_fused_cancellable(jobs, cancel, status)
+    e1.record()
+    time.sleep(full_ms / 4e3)
+    cancel.value = 1
+    torch.cuda.synchronize()
+    assert status.value in (1, 2)
+    if status.value == 2:
+        assert e0.elapsed_time(e1) < full_ms
+    # the next launch is whole again
+    cancel.value = 0
+    for j in jobs:
+        j.cap.zero_()
+    glc.commit.commit_batch_fused(jobs)
+    assert all((from_dev(j.cap) == w).all() for j, w in zip(jobs, want))
+    assert glc.commit.fused_timeouts() == 0
+    cancel.close()
+    status.close()
+
+
 def test_commit_batch_fused_contract(glc, syn):
     job, _ = make_job(glc, syn, 17, 1, 1, 4, "fused-big")
     with pytest.raises(glc.GlcError):

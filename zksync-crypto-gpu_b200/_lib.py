@@ -59,6 +59,9 @@ SIGNATURES = {
     "glc_commit_batch": (C.c_int, [vp, u32, u32, vp]),
     "glc_commit_batch_fused": (C.c_int, [vp, u32, vp]),
     "glc_commit_batch_fused_traced": (C.c_int, [vp, u32, u64p, u64, vp]),
+    "glc_commit_batch_fused_cancellable": (C.c_int, [vp, u32, vp, vp, vp]),
+    "glc_mapped_word_create": (C.c_int, [vp, vp]),
+    "glc_mapped_word_destroy": (C.c_int, [vp]),
     "glc_commit_batch_fused_timeouts": (C.c_int, [vp]),
     "glc_commit_graph_create": (C.c_int, [vp, u32, u32, vp]),
     "glc_commit_graph_launch": (C.c_int, [vp, vp]),

@@ -75,6 +75,46 @@ def commit_batch(jobs: list[CommitJob], n_streams: int = 0, stream=None) -> None
     call("glc_commit_batch", C.addressof(arr) if jobs else None, len(jobs), n_streams, stream_handle(stream))
 
 
+class MappedWord:
+    """A 32-bit word of page-locked host memory mapped into the device (glc_mapped_word_create):
+    `value` reads and writes it from the host, `device` is its address for kernels."""
+
+    def __init__(self):
+        h, d = C.c_void_p(), C.c_void_p()
+        call("glc_mapped_word_create", C.byref(h), C.byref(d))
+        self._host, self.device = h.value, d.value
+        self._word = C.c_uint32.from_address(self._host)
+
+    @property
+    def value(self) -> int:
+        return self._word.value
+
+    @value.setter
+    def value(self, v: int) -> None:
+        self._word.value = v
+
+    def close(self) -> None:
+        if self._host:
+            call("glc_mapped_word_destroy", self._host)
+            self._host = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def commit_batch_fused_cancellable(jobs: list[CommitJob], cancel: MappedWord, status: MappedWord | None = None,
+                                   stream=None) -> None:
+    """commit_batch_fused that stops claiming and starting items once `cancel.value` is non-zero
+    (glc_commit_batch_fused_cancellable); `status.value` becomes 1 when every item ran, 2 when a
+    cancel skipped some (outputs incomplete)."""
+    arr = _array(jobs)
+    call("glc_commit_batch_fused_cancellable", C.addressof(arr) if jobs else None, len(jobs), cancel.device,
+         status.device if status is not None else None, stream_handle(stream))
+
+
 def commit_batch_fused(jobs: list[CommitJob], stream=None, trace=None) -> None:
     """Many small commitments (2^log_n <= 2^16 rows each) in ONE persistent launch
     (glc_commit_batch_fused): work items of every stage of every job, each waiting only for the

@@ -99,11 +99,13 @@ static constexpr uint32_t FUSED_WAIT_LIMIT = 1u << 22;  // x 200 ns sleeps: abou
 __global__ void __launch_bounds__(FUSED_THREADS, 3)
     fused_commit_kernel(const FusedEntry *entries, uint32_t n_entries, uint64_t total_units, uint32_t *counters,
                         uint32_t *abort_flag, unsigned long long *next_unit, unsigned long long *trace,
-                        uint64_t trace_items) {
+                        uint64_t trace_items, const volatile uint32_t *cancel, uint32_t *status) {
   extern __shared__ uint64_t smem[];
   __shared__ uint64_t s_unit;
-  __shared__ uint32_t s_entry;
+  __shared__ uint32_t s_entry, s_skip;
   const uint32_t tid = threadIdx.x;
+  // launch-wide words after the abort flag: CTAs that have left, and whether a cancel skipped items
+  uint32_t *exited = abort_flag + 1, *cancelled = abort_flag + 2;
   // Thread 0 claims the CTA's next item while the current one runs, so the claim's round trip
   // to L2 is off the critical path.  Progress still holds: a CTA's claims increase, so the CTA
   // that holds the lowest unfinished item is running it (its claimed-next item is above it),
@@ -114,7 +116,16 @@ __global__ void __launch_bounds__(FUSED_THREADS, 3)
     __syncthreads();  // the previous item's last reads of s_unit, s_entry and shared memory are done
     if (tid == 0) {
       s_unit = claimed;
-      if (claimed < total_units) claimed = atomicAdd(next_unit, 1ull);
+      if (claimed < total_units) {
+        if (cancel && *cancel) {
+          // cancelled: claim nothing more, skip this item, and end every wait of the launch
+          atomicExch(cancelled, 1u);
+          atomicExch(abort_flag, 1u);
+          s_unit = total_units;
+        } else {
+          claimed = atomicAdd(next_unit, 1ull);
+        }
+      }
     }
     __syncthreads();
     const uint64_t u = s_unit;
@@ -137,20 +148,29 @@ __global__ void __launch_bounds__(FUSED_THREADS, 3)
     }
     __syncthreads();
     const FusedEntry &E = entries[s_entry];
-    if (tid == 0 && E.dep != NO_COUNTER) {
-      // after one expired wait (a bug, not a slow producer) no item waits any more: the launch
-      // then ends within one wait limit whatever else is wrong
-      uint32_t it = 0;
-      while (ld_acquire(counters + E.dep) < E.dep_target && !ld_acquire(abort_flag)) {
-        if (++it > FUSED_WAIT_LIMIT) {
-          atomicAdd(&g_fused_timeouts, 1ull);
-          atomicExch(abort_flag, 1u);
-          break;
+    if (tid == 0) {
+      if (E.dep != NO_COUNTER) {
+        // after one expired wait (a bug, not a slow producer) no item waits any more: the launch
+        // then ends within one wait limit whatever else is wrong
+        uint32_t it = 0;
+        while (ld_acquire(counters + E.dep) < E.dep_target && !ld_acquire(abort_flag)) {
+          if (++it > FUSED_WAIT_LIMIT) {
+            atomicAdd(&g_fused_timeouts, 1ull);
+            atomicExch(abort_flag, 1u);
+            break;
+          }
+          if (cancel && (it & 63) == 0 && *cancel) {
+            atomicExch(cancelled, 1u);
+            atomicExch(abort_flag, 1u);
+          }
+          __nanosleep(200);
         }
-        __nanosleep(200);
       }
+      // a cancelled launch skips the items it has not started (their inputs may be incomplete)
+      s_skip = cancel && ld_acquire(cancelled) ? 1u : 0u;
     }
     __syncthreads();  // the acquire above orders the producers' writes before this CTA's reads
+    if (s_skip) break;
     const unsigned long long t_start = (trace && tid == 0) ? global_ns() : 0ull;
     const uint64_t local = u - E.first;
     const uint32_t kind = E.kind;
@@ -202,6 +222,14 @@ __global__ void __launch_bounds__(FUSED_THREADS, 3)
       }
       if (E.done1 != NO_COUNTER) red_release_add(counters + E.done1, 1u);
       if (E.done2 != NO_COUNTER) red_release_add(counters + E.done2, 1u);
+    }
+  }
+  // the last CTA to leave reports how the launch ended: 1 = every item ran, 2 = cancelled
+  if (status && tid == 0) {
+    __threadfence();
+    if (atomicAdd(exited, 1u) == gridDim.x - 1) {
+      *reinterpret_cast<volatile uint32_t *>(status) = ld_acquire(cancelled) ? 2u : 1u;
+      __threadfence_system();
     }
   }
 }
@@ -471,7 +499,7 @@ void fused_forget_device(int dev) {
 using namespace glc;
 
 static glc_status commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs, unsigned long long *trace,
-                                     uint64_t trace_items, void *stream_) {
+                                     uint64_t trace_items, const uint32_t *cancel, uint32_t *status, void *stream_) {
   if (n_jobs == 0) return 0;
   if (!jobs) return fail("commit_batch_fused: null jobs");
   for (uint32_t i = 0; i < n_jobs; i++) {
@@ -495,7 +523,7 @@ static glc_status commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs
   if (per_sm < 1) return fail("commit_batch_fused: the kernel does not fit on an SM");
   // one stream-ordered buffer: the entries, then the counters and the item counter (zeroed)
   const size_t eb = P.entries.size() * sizeof(FusedEntry);
-  const size_t cb = ((P.target.size() + 1) * sizeof(uint32_t) + 7) / 8 * 8 + sizeof(unsigned long long);
+  const size_t cb = ((P.target.size() + 3) * sizeof(uint32_t) + 7) / 8 * 8 + sizeof(unsigned long long);
   if (dev < 0 || dev >= MAX_DEVICES) return fail("commit_batch_fused: device ordinal out of range");
   cudaMemPool_t pool = nullptr;
   ce = fused_pool(dev, &pool);
@@ -513,8 +541,9 @@ static glc_status commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs
     unsigned long long *next = reinterpret_cast<unsigned long long *>(buf + eb + cb - sizeof(unsigned long long));
     uint32_t ne = (uint32_t)P.entries.size();
     uint64_t tu = total;
-    void *args[] = {(void *)&de,   (void *)&ne,   (void *)&tu,         (void *)&counters, (void *)&abort_flag,
-                    (void *)&next, (void *)&trace, (void *)&trace_items};
+    const volatile uint32_t *cancel_v = cancel;
+    void *args[] = {(void *)&de,   (void *)&ne,    (void *)&tu,          (void *)&counters, (void *)&abort_flag,
+                    (void *)&next, (void *)&trace, (void *)&trace_items, (void *)&cancel_v, (void *)&status};
     ce = cudaLaunchCooperativeKernel((const void *)fused_commit_kernel, dim3((unsigned)(per_sm * sms)),
                                      dim3(FUSED_THREADS), args, P.smem, stream);
     count_launches(1);
@@ -524,14 +553,42 @@ static glc_status commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs
 }
 
 extern "C" glc_status glc_commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs, void *stream) {
-  return commit_batch_fused(jobs, n_jobs, nullptr, 0, stream);
+  return commit_batch_fused(jobs, n_jobs, nullptr, 0, nullptr, nullptr, stream);
 }
 
 extern "C" glc_status glc_commit_batch_fused_traced(const glc_commit_job *jobs, uint32_t n_jobs, uint64_t *trace,
                                                     uint64_t trace_items, void *stream) {
   if (!trace && trace_items) return fail("commit_batch_fused_traced: null trace buffer");
-  return commit_batch_fused(jobs, n_jobs, reinterpret_cast<unsigned long long *>(trace), trace_items, stream);
+  return commit_batch_fused(jobs, n_jobs, reinterpret_cast<unsigned long long *>(trace), trace_items, nullptr, nullptr,
+                            stream);
 }
+
+extern "C" glc_status glc_commit_batch_fused_cancellable(const glc_commit_job *jobs, uint32_t n_jobs,
+                                                         const uint32_t *cancel, uint32_t *status, void *stream) {
+  if (!cancel) return fail("commit_batch_fused_cancellable: null cancel word");
+  return commit_batch_fused(jobs, n_jobs, nullptr, 0, cancel, status, stream);
+}
+
+extern "C" glc_status glc_mapped_word_create(uint32_t **host, uint32_t **device) {
+  if (!host || !device) return fail("mapped_word_create: null output");
+  *host = nullptr;
+  *device = nullptr;
+  uint32_t *h = nullptr;
+  cudaError_t e = cudaHostAlloc((void **)&h, sizeof(uint32_t), cudaHostAllocMapped);
+  if (e != cudaSuccess) return (int)e;
+  *h = 0;
+  uint32_t *d = nullptr;
+  e = cudaHostGetDevicePointer((void **)&d, h, 0);
+  if (e != cudaSuccess) {
+    cudaFreeHost(h);
+    return (int)e;
+  }
+  *host = h;
+  *device = d;
+  return 0;
+}
+
+extern "C" glc_status glc_mapped_word_destroy(uint32_t *host) { return host ? (int)cudaFreeHost(host) : 0; }
 
 extern "C" glc_status glc_commit_batch_fused_timeouts(uint64_t *out) {
   if (!out) return fail("commit_batch_fused_timeouts: null output");

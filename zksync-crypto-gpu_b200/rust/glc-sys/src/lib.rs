@@ -169,6 +169,10 @@ extern "C" {
     pub fn glc_commit_batch_fused(jobs: *const glc_commit_job, n_jobs: u32, stream: Stream) -> GlcStatus;
     pub fn glc_commit_batch_fused_traced(jobs: *const glc_commit_job, n_jobs: u32, trace: *mut u64,
         trace_items: u64, stream: Stream) -> GlcStatus;
+    pub fn glc_commit_batch_fused_cancellable(jobs: *const glc_commit_job, n_jobs: u32, cancel: *const u32,
+        status: *mut u32, stream: Stream) -> GlcStatus;
+    pub fn glc_mapped_word_create(host: *mut *mut u32, device: *mut *mut u32) -> GlcStatus;
+    pub fn glc_mapped_word_destroy(host: *mut u32) -> GlcStatus;
     pub fn glc_commit_batch_fused_timeouts(out: *mut u64) -> GlcStatus;
     pub fn glc_commit_graph_create(jobs: *const glc_commit_job, n_jobs: u32, n_streams: u32,
         out: *mut *mut glc_graph) -> GlcStatus;
