@@ -238,36 +238,45 @@ __global__ void __launch_bounds__(FUSED_THREADS, 3)
 // with its dependency counter) and the launch of the persistent grid.
 struct FusedPlan {
   std::vector<FusedEntry> entries;
-  std::vector<uint32_t> target;  // per counter: the items that count into it
-  std::vector<std::vector<FusedEntry>> stages;
+  std::vector<uint32_t> target;       // per counter: the items that count into it
+  std::vector<size_t> stage_begin;    // index in `entries` of each stage's first entry
   size_t smem = 0;
 
   uint32_t counter() {
     target.push_back(0);
     return (uint32_t)target.size() - 1;
   }
-  void begin_stage() { stages.emplace_back(); }
+  void begin_stage() { stage_begin.push_back(entries.size()); }
   void add(FusedEntry e, uint32_t dep, uint32_t done1, uint32_t done2 = NO_COUNTER) {
     e.dep = dep;
     e.done1 = done1;
     e.done2 = done2;
     if (done1 != NO_COUNTER) target[done1] += (uint32_t)e.units;
     if (done2 != NO_COUNTER) target[done2] += (uint32_t)e.units;
-    if (e.units) stages.back().push_back(e);
+    if (e.units) entries.push_back(e);
   }
   // Heaviest items of each stage first (the last items to start bound a stage's tail), then the
-  // global numbering and the wait targets.
+  // global numbering and the wait targets.  Sorts indexes, then moves each entry once.
   uint64_t finish() {
+    std::vector<FusedEntry> out;
+    out.reserve(entries.size());
+    std::vector<uint32_t> order;
     uint64_t first = 0;
-    for (auto &st : stages) {
-      std::stable_sort(st.begin(), st.end(), [](const FusedEntry &x, const FusedEntry &y) { return cost(x) > cost(y); });
-      for (FusedEntry &e : st) {
-        e.first = first;
-        first += e.units;
-        e.dep_target = e.dep == NO_COUNTER ? 0 : target[e.dep];
-        entries.push_back(e);
+    for (size_t s = 0; s < stage_begin.size(); s++) {
+      const size_t b = stage_begin[s], e = s + 1 < stage_begin.size() ? stage_begin[s + 1] : entries.size();
+      order.resize(e - b);
+      for (size_t i = b; i < e; i++) order[i - b] = (uint32_t)i;
+      std::stable_sort(order.begin(), order.end(),
+                       [&](uint32_t x, uint32_t y) { return cost(entries[x]) > cost(entries[y]); });
+      for (uint32_t i : order) {
+        FusedEntry &x = entries[i];
+        x.first = first;
+        first += x.units;
+        x.dep_target = x.dep == NO_COUNTER ? 0 : target[x.dep];
+        out.push_back(x);
       }
     }
+    entries.swap(out);
     return first;
   }
   static uint64_t cost(const FusedEntry &e) {
@@ -303,7 +312,7 @@ static FusedEntry ntt_entry(const DeviceTables *t, uint32_t log_n, uint32_t q, u
                             bool inverse, uint32_t log_ext, uint32_t coset, size_t &smem) {
   FusedEntry e{};
   e.kind = FK_NTT;
-  NttTuning tu = ntt_tuning(log_n);
+  NttTuning tu{};  // the fused items use radix-16 rounds; make_pass reads nothing else from it here
   tu.radix_bits = 4;
   const PassShape sh = make_pass(e.ntt, t, tu, ps, q, np, in, out, in_stride, out_stride, cols, log_n, false, inverse,
                                  log_ext, coset, 1);
