@@ -596,7 +596,7 @@ def uneven_batch(glc, torch, budget_gb=120.0, streams=8, with_reference=True, jo
     waves.append(cur)
     stream = torch.cuda.current_stream()
     t = {"plain": 0.0, "batched": 0.0, "graph": 0.0, "fused": 0.0, "reference_kernels": 0.0}
-    fused = all(l <= 16 for l, _, _, _ in jobs)
+    fused = all(l <= 22 for l, _, _, _ in jobs)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     try:
         import refkern
@@ -623,8 +623,7 @@ def uneven_batch(glc, torch, budget_gb=120.0, streams=8, with_reference=True, jo
         graph.launch()
         torch.cuda.synchronize()
         caps_graph = [jb.cap.clone() for jb in bufs]
-        # the fused form (one cooperative launch for every stage of every job) takes waves of
-        # jobs of at most 2^16 rows
+        # the fused form: one cooperative launch for every stage of every job of the wave
         forms = ("plain", "batched", "graph") + (("fused",) if fused else ())
         if fused:
             glc.commit.commit_batch_fused(bufs, stream)

@@ -196,7 +196,7 @@ glc_status glc_commit_cap_noalloc(const uint64_t *evals, uint64_t evals_stride, 
  * Capturable into a CUDA graph. */
 glc_status glc_commit_batch(const glc_commit_job *jobs, uint32_t n_jobs, uint32_t n_streams, void *stream);
 
-/* Many small commitments (log_n <= 16 each) in ONE launch: a persistent grid (launched
+/* Many commitments (log_n <= 22 each) in ONE launch: a persistent grid (launched
  * cooperatively, so all its CTAs are resident) takes work items of every stage of every job
  * (inverse NTT tiles, bit reversal, coset NTT tiles, leaves, node layers, caps) from a global
  * counter in stage order; each item waits (bounded, about 1 s) only for the items it reads from,

@@ -202,8 +202,30 @@ def test_commit_batch_fused_cancellable(glc, syn):
     status.close()
 
 
+def test_commit_batch_fused_large_jobs(glc, syn):
+    """Jobs of 2^17..2^22 rows (strided first passes of 5..10 stages on 2^12-element tiles) mixed
+    with small ones in one launch: every LDE, tree and cap equals glc_commit's."""
+    shapes = [(22, 8, 1, 4), (20, 24, 2, 4), (17, 40, 1, 4), (19, 8, 2, 5), (12, 16, 1, 4), (21, 9, 1, 3)]
+    jobs = [make_job(glc, syn, l, c, e, cap, "flarge-%d" % i, keep_monomials=(i % 2 == 0))[0]
+            for i, (l, c, e, cap) in enumerate(shapes)]
+    glc.commit.commit_batch_fused(jobs)
+    got = [(from_dev(j.lde).copy(), from_dev(j.trees).copy(), from_dev(j.cap).copy()) for j in jobs]
+    for j in jobs:
+        j.cap.zero_()
+        j.trees.zero_()
+        glc.commit.commit(j)
+    for j, (lde, trees, cap) in zip(jobs, got):
+        n, f = 1 << j.log_n, 1 << j.log_lde
+        computed = 8 * n - 4 * (1 << (j.log_cap - j.log_lde))  # the tree prefix below the cap
+        t = from_dev(j.trees).reshape(f, 8 * n)[:, :computed]
+        assert (canon(from_dev(j.lde)) == canon(lde)).all(), (j.log_n, "lde")
+        assert (canon(t) == canon(trees.reshape(f, 8 * n)[:, :computed])).all(), (j.log_n, "trees")
+        assert (from_dev(j.cap) == cap).all(), (j.log_n, "cap")
+    assert glc.commit.fused_timeouts() == 0
+
+
 def test_commit_batch_fused_contract(glc, syn):
-    job, _ = make_job(glc, syn, 17, 1, 1, 4, "fused-big")
+    job, _ = make_job(glc, syn, 23, 1, 1, 4, "fused-big")
     with pytest.raises(glc.GlcError):
         glc.commit.commit_batch_fused([job])
     glc.commit.commit_batch_fused([])  # nothing to do

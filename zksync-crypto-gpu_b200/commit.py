@@ -3,7 +3,7 @@
 The sequence shivini runs around boojum-cuda for one commitment
 (crates/shivini/src/data_structures/storage.rs:155-330, cache.rs:353-418), as one call
 (glc_commit), as a batch of uneven jobs on concurrent streams (glc_commit_batch), or as a
-captured CUDA graph replayed with one launch (CommitGraph), or, for jobs of at most 2^16 rows, as
+captured CUDA graph replayed with one launch (CommitGraph), or, for jobs of at most 2^22 rows, as
 one persistent cooperative launch that runs every stage of every job (commit_batch_fused).
 """
 from __future__ import annotations
@@ -116,7 +116,7 @@ def commit_batch_fused_cancellable(jobs: list[CommitJob], cancel: MappedWord, st
 
 
 def commit_batch_fused(jobs: list[CommitJob], stream=None, trace=None) -> None:
-    """Many small commitments (2^log_n <= 2^16 rows each) in ONE persistent launch
+    """Many commitments (2^log_n <= 2^22 rows each) in ONE persistent launch
     (glc_commit_batch_fused): work items of every stage of every job, each waiting only for the
     items it reads from.  `trace`: a device buffer of 4 * N 8-byte words, cleared by the caller,
     that receives the per-item records of the first N items (glc_commit_batch_fused_traced; see

@@ -3,7 +3,8 @@
 // The per-call form issues about 28 kernels per commitment (NTT passes, bit reversal, one leaf
 // launch and node layers per coset, the cap gather); for jobs of 2^12..2^16 rows each of those
 // kernels runs for microseconds and cannot fill 148 SMs, so a batch of such jobs is bound by
-// launch latency and by the tails of small grids (the reference's per-stage and per-layer
+// launch latency and by the tails of small grids; jobs up to 2^22 rows (two NTT passes on
+// 2^12-element tiles whose rows stay at least 4 elements = 32 bytes wide) run in the same launch (the reference's per-stage and per-layer
 // launches, crates/boojum-cuda/src/ntt.rs:201-241 and src/poseidon2.rs:276-295, are the same
 // shape).  Here a persistent grid (as many CTAs as fit on the device at once, launched
 // cooperatively so that all of them are resident) takes work items from one global counter, in
@@ -12,10 +13,10 @@
 //   that transforms the monomials in place last, after the others have read them) -> leaf
 //   hashes -> node layer 1, 2, ... -> cap gather,
 // every stage listing the items of all jobs, heaviest first.  An item is an NTT tile of 2^12
-// elements (or a whole column of a smaller NTT) in up to two columns, 4096 rows of a bit reversal,
-// 256 leaves, 256 nodes or 256 cap entries: large enough that the per-item costs (the claim of
-// the item number, the search for its entry, the dependency check and the release of its count,
-// a few microseconds together) stay a few percent of its work.  Before it runs, an item waits
+// elements (or a whole column of a smaller NTT) in up to 4 columns (8 from 2^17 rows), 4096
+// rows of a bit reversal, 256 leaves, 256 nodes or 256 cap entries: large enough that the
+// per-item costs (the claim of the item number, the search for its entry, the dependency check
+// and the release of its count, a few microseconds together) stay a few percent of its work.  Before it runs, an item waits
 // until the items it reads from are done: each stage of each job (per coset where it applies)
 // counts its finished items, and the item waits for its producer's count to reach the producer's
 // item total.  Items wait only for items that come earlier in the order, which some resident CTA
@@ -40,9 +41,12 @@ namespace glc {
 namespace cg = cooperative_groups;
 
 static constexpr uint32_t FUSED_THREADS = 256;
-static constexpr uint32_t FUSED_MAX_LOG_N = 16;
-// columns per NTT item (fewer when a job has fewer)
-static constexpr uint32_t FUSED_NTT_COLS = 2;
+static constexpr uint32_t FUSED_MAX_LOG_N = 22;  // two passes of at most 12 stages on 2^12-element tiles with rows of >= 4 elements
+// columns per NTT item (fewer when a job has fewer): each item rebuilds its tile's block
+// twiddles, so more columns amortise them; jobs from 2^17 rows have items to spare.  Measured on
+// the uneven batch: 2 / 4 columns: small jobs 20.7 / 20.4 ms; 8 columns from 2^17 rows: the
+// 300 jobs 4851 -> 4726 ms.
+static constexpr uint32_t FUSED_NTT_COLS = 4, FUSED_NTT_COLS_LARGE = 8, FUSED_LARGE_LOG_N = 17;
 // rows of one column per bit-reversal item
 static constexpr uint32_t FUSED_BITREV_ROWS = 4096;
 
@@ -316,8 +320,8 @@ static FusedEntry ntt_entry(const DeviceTables *t, uint32_t log_n, uint32_t q, u
   tu.radix_bits = 4;
   const PassShape sh = make_pass(e.ntt, t, tu, ps, q, np, in, out, in_stride, out_stride, cols, log_n, false, inverse,
                                  log_ext, coset, 1);
-  // the batch fills the device together: FUSED_NTT_COLS columns per item whatever the job's size
-  e.ntt.cols_per_cta = std::min(FUSED_NTT_COLS, cols);
+  // the batch fills the device together: the item width does not shrink for small batches
+  e.ntt.cols_per_cta = std::min(log_n >= FUSED_LARGE_LOG_N ? FUSED_NTT_COLS_LARGE : FUSED_NTT_COLS, cols);
   e.tiles_per_col = sh.tiles_per_col;
   e.units = sh.tiles_per_col * ((cols + e.ntt.cols_per_cta - 1) / e.ntt.cols_per_cta);
   smem = std::max(smem, sh.smem);
@@ -514,7 +518,7 @@ static glc_status commit_batch_fused(const glc_commit_job *jobs, uint32_t n_jobs
   for (uint32_t i = 0; i < n_jobs; i++) {
     const int e = commit_check(jobs[i]);
     if (e) return e;
-    if (jobs[i].log_n > FUSED_MAX_LOG_N) return fail("commit_batch_fused: log_n must be <= 16");
+    if (jobs[i].log_n > FUSED_MAX_LOG_N) return fail("commit_batch_fused: log_n must be <= 22");
   }
   const DeviceTables *t = current_tables();
   if (!t) return fail("commit_batch_fused: glc_context_create has not been called on this device");
