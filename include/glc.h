@@ -83,6 +83,10 @@ glc_status glc_bit_reverse_in_place(uint64_t *values, uint64_t stride, uint32_t 
  * generates them from boojum at build time (crates/boojum-cuda/build/poseidon2_gl.rs:3,34);
  * without this call the library uses its built-in placeholder set. */
 glc_status glc_poseidon2_set_round_constants(const uint64_t *round_constants);
+/* *out = 1 when glc_poseidon2_set_round_constants has installed constants on the current device,
+ * 0 while every digest (leaves, nodes, trees, commitments, caps) still uses the built-in
+ * placeholder set, which is not boojum's.  Host-side bookkeeping only; launches nothing. */
+glc_status glc_poseidon2_round_constants_installed(uint32_t *out);
 /* Replaces GpuTreeHasher::compute_leaf_hashes (poseidon2.rs:180-226). */
 glc_status glc_poseidon2_compute_leaf_hashes(const uint64_t *values, size_t values_len, uint64_t *results,
                                              size_t results_len, uint32_t log_rows_per_hash, bool load_intermediate,
@@ -165,7 +169,9 @@ typedef struct glc_commit_job {
   uint64_t *cap;          /* [4][2^log_cap]: the subtree caps concatenated coset by coset */
 } glc_commit_job;
 
-/* One commitment on one stream (the plain per-call form). */
+/* One commitment on one stream (the plain per-call form).  Its digests use the round constants
+ * of glc_poseidon2_set_round_constants (glc_poseidon2_round_constants_installed tells whether the
+ * placeholder set is still in use). */
 glc_status glc_commit(const glc_commit_job *job, void *stream);
 
 /* glc_commit that also records CUDA events (cudaEvent_t, created by the caller) at the stage

@@ -71,3 +71,12 @@ def test_header_compiles_as_c_and_links(tmp_path):
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout, r.stderr)
+
+
+def test_round_constants_query_without_a_device():
+    """The installed-constants query is host bookkeeping: it answers without a GPU, and a process
+    that never called glc_poseidon2_set_round_constants reports the placeholder set."""
+    g = load_package()
+    assert g.poseidon2.round_constants_installed() is False
+    L = g._lib.lib()
+    assert L.glc_poseidon2_round_constants_installed(None) == 1

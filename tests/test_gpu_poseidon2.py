@@ -18,6 +18,11 @@ def glc(round_constants):
     ctx.destroy()
 
 
+def test_round_constants_installed(glc):
+    """After set_round_constants the device reports its constants installed."""
+    assert glc.poseidon2.round_constants_installed() is True
+
+
 @pytest.mark.parametrize("log_n", [0, 4, 12])
 @pytest.mark.parametrize("checkpointed", [False, True])
 @pytest.mark.parametrize("cols,log_rows", [(9, 1), (8, 0), (1, 0), (17, 0), (3, 3)])

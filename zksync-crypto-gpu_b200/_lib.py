@@ -41,6 +41,7 @@ SIGNATURES = {
     "glc_bit_reverse": (C.c_int, [u64p, u64, u64p, u64, u32, u32, vp]),
     "glc_bit_reverse_in_place": (C.c_int, [u64p, u64, u32, u32, vp]),
     "glc_poseidon2_set_round_constants": (C.c_int, [u64p]),
+    "glc_poseidon2_round_constants_installed": (C.c_int, [vp]),
     "glc_poseidon2_compute_leaf_hashes": (C.c_int, [u64p, sz, u64p, sz, u32, b, b, vp]),
     "glc_poseidon2_compute_node_hashes": (C.c_int, [u64p, sz, u64p, sz, vp]),
     "glc_poseidon2_build_merkle_tree_leaves": (C.c_int, [u64p, sz, u64p, sz, u32, b, b, vp]),

@@ -614,6 +614,12 @@ extern "C" glc_status glc_poseidon2_set_round_constants(const uint64_t *round_co
   return p2_install_round_constants(round_constants);
 }
 
+extern "C" glc_status glc_poseidon2_round_constants_installed(uint32_t *out) {
+  if (!out) return fail("poseidon2: null output");
+  *out = p2_constants_installed() ? 1u : 0u;
+  return 0;
+}
+
 extern "C" glc_status glc_poseidon2_compute_leaf_hashes(const uint64_t *values, size_t values_len, uint64_t *results,
                                                         size_t results_len, uint32_t log_rows_per_hash,
                                                         bool load_intermediate, bool store_intermediate,

@@ -17,6 +17,14 @@ def set_round_constants(round_constants) -> None:
     call("glc_poseidon2_set_round_constants", C.addressof(arr))
 
 
+def round_constants_installed() -> bool:
+    """True once set_round_constants has run on the current device; until then every digest uses
+    the library's built-in placeholder constants (glc_poseidon2_round_constants_installed)."""
+    v = C.c_uint32()
+    call("glc_poseidon2_round_constants_installed", C.byref(v))
+    return bool(v.value)
+
+
 class GLHasher:
     RATE = 8
     CAPACITY = 4

@@ -126,6 +126,7 @@ extern "C" {
 
     // GpuTreeHasher for GLHasher (crates/boojum-cuda/src/poseidon2.rs:180-380)
     pub fn glc_poseidon2_set_round_constants(round_constants: *const u64) -> GlcStatus;
+    pub fn glc_poseidon2_round_constants_installed(out: *mut u32) -> GlcStatus;
     pub fn glc_poseidon2_compute_leaf_hashes(values: *const u64, values_len: usize, results: *mut u64,
         results_len: usize, log_rows_per_hash: u32, load_intermediate: bool, store_intermediate: bool,
         stream: Stream) -> GlcStatus;
